@@ -1,0 +1,158 @@
+/*
+ * mag_c.h -- C ABI of libmag_b200.so, the B200 (sm_100a) implementation of
+ * mag's constrained hybrid Monte Carlo path for SU(3) gauge fields.
+ *
+ * The reference (hummingtree/mag) exposes this path as free inline C++
+ * functions over qlat::Field<cps::Matrix> (field-hmc.h, field-matrix.h,
+ * field-multi.h, field-wloop.h, field-demon.h).  Each entry point below names
+ * the reference function it replaces.  include/mag_field.hpp forwards the
+ * reference names to these entry points for C++ drivers.
+ *
+ * Conventions
+ *  - Every call returns int: MAG_OK (0) or a negative MAG_ERR_* code; no
+ *    exception crosses the ABI (the reference asserts and aborts instead).
+ *  - Host fields are AoS double[V][4][3][3][2] (site, mu, row, column, re/im),
+ *    site index x0 + L0*(x1 + L1*(x2 + L2*x3)) as qlat's index_from_coordinate;
+ *    momenta and forces use the same layout (Hermitian traceless matrices).
+ *  - A context owns its device memory and one CUDA stream; it is not
+ *    thread-safe (one host thread per context).  It holds one lattice or an
+ *    ensemble of independent chains that advance in lockstep.
+ *  - All randomness is Philox-4x32-10 keyed by (seed + chain index); a
+ *    validation run may instead supply momenta and uniforms from the host.
+ */
+#ifndef MAG_C_H
+#define MAG_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MAG_OK 0
+#define MAG_ERR_ARG (-1)        /* invalid argument */
+#define MAG_ERR_CUDA (-2)       /* CUDA runtime error (message: mag_last_error) */
+#define MAG_ERR_NAN (-3)        /* NaN/Inf detected in a result */
+#define MAG_ERR_STATE (-4)      /* call not valid in the current state */
+#define MAG_ERR_NOMEM (-5)      /* device allocation failed */
+
+enum { MAG_ACTION_WILSON = 0, MAG_ACTION_IWASAKI = 1 };           /* qlat::Gauge::type */
+enum { MAG_PREC_FP64 = 0, MAG_PREC_MIXED = 1 };
+enum { MAG_INT_FORCE_GRADIENT = 0, MAG_INT_LEAPFROG = 1 };
+enum { MAG_ACCEPT_METROPOLIS = 0, MAG_ACCEPT_DEMON = 1 };
+
+/* Arg_chmc (field-hmc.h:294-307) plus qlat::Gauge and the B200 run options. */
+typedef struct mag_params {
+    int dims[4];          /* lattice extents L0..L3 (each >= 2, divisible by mag) */
+    int mag;              /* Arg_chmc::mag; 0 = unconstrained */
+    int action;           /* MAG_ACTION_* */
+    double beta;          /* Arg_chmc::beta */
+    double c1;            /* Gauge::c1 (Iwasaki -0.331); c0 = 1 - 8 c1 */
+    double rho;           /* stout parameter */
+    int n_stout;          /* stout levels (0 = thin links) */
+    double tau;           /* trajectory length; dt = tau / n_steps (Arg_chmc::dt) */
+    int n_steps;          /* Arg_chmc::trajectory_length */
+    int precision;        /* MAG_PREC_* */
+    int integrator;       /* MAG_INT_* */
+    int accept;           /* MAG_ACCEPT_* */
+    double e_max;         /* demon window */
+    int n_forced_accept;  /* Arg_chmc::num_forced_accept_step */
+    uint64_t seed;        /* Philox key of chain 0 */
+} mag_params;
+
+/* One trajectory of one chain (the summary row of field-hmc.h:845-864). */
+typedef struct mag_traj_result {
+    double h_old, h_new, delta_h;
+    double kinetic_old, kinetic_new, action_old, action_new;
+    double plaq_sum_old, plaq_sum_new, rect_sum_old, rect_sum_new;
+    double uniform;
+    double demon[2];
+    double reunit_maxdev;
+    double avg_plaquette;
+    int accept;
+    int traj;
+} mag_traj_result;
+
+typedef struct mag_ctx mag_ctx;
+
+/* -------------------------------------------------------------- lifecycle */
+/* run_chmc's field set-up (field-hmc.h:775-784) for one lattice */
+int mag_ctx_create(const mag_params* p, mag_ctx** out);
+/* an ensemble of n independent chains (per-chain dims, mag, beta, c1, rho);
+   precision, integrator, accept, n_stout, tau, n_steps and seed come from p[0] */
+int mag_ensemble_create(const mag_params* p, int n_chains, mag_ctx** out);
+int mag_ctx_destroy(mag_ctx* ctx);
+const char* mag_last_error(void);
+int mag_ctx_num_chains(const mag_ctx* ctx, int* n);
+int mag_ctx_device_bytes(const mag_ctx* ctx, size_t* bytes);
+
+/* ------------------------------------------------------------- field I/O */
+/* copy a host configuration in / out (replaces gField = gFieldExt copies) */
+int mag_gauge_set(mag_ctx* ctx, int chain, const double* host_aos);
+int mag_gauge_get(mag_ctx* ctx, int chain, double* host_aos);
+/* Haar-random hot start from Philox (seed + chain) / unit links */
+int mag_gauge_hot_start(mag_ctx* ctx, uint64_t seed);
+int mag_gauge_cold_start(mag_ctx* ctx);
+/* momenta: init_momentum (field-hmc.h:675-693) from the host or from Philox */
+int mag_momentum_set(mag_ctx* ctx, int chain, const double* host_aos);
+int mag_momentum_get(mag_ctx* ctx, int chain, double* host_aos);
+int mag_momentum_refresh(mag_ctx* ctx, uint64_t traj);
+/* Metropolis uniforms for the next trajectory, one per chain (u_rand_gen, field-hmc.h:818);
+   pass NULL to return to the Philox stream */
+int mag_uniforms_set(mag_ctx* ctx, const double* u);
+
+/* ------------------------------------------------------------- operators */
+/* get_force (field-hmc.h:339-425) on the current links, smeared if n_stout > 0 */
+int mag_gauge_force(mag_ctx* ctx, int chain, double* host_force_aos);
+/* get_extended_staple_dagger (field-hmc.h:262-269) for every link of the
+   (smeared) links */
+int mag_staple(mag_ctx* ctx, int chain, double* host_staple_aos);
+/* total_plaq / total_rectangular (field-matrix.h:299-385) of the smeared
+   links and the gauge action (field-hmc.h:632-639) */
+int mag_action(mag_ctx* ctx, int chain, double* plaq_sum, double* rect_sum, double* action);
+/* avg_plaquette (field-matrix.h:387-389) of the thin links */
+int mag_plaquette(mag_ctx* ctx, int chain, double* avg);
+/* kinetic part of get_hamiltonian (field-hmc.h:596-629) */
+int mag_kinetic(mag_ctx* ctx, int chain, double* kinetic);
+/* get_hamiltonian (field-hmc.h:589-644): out = {H, kinetic, action} */
+int mag_hamiltonian(mag_ctx* ctx, int chain, double out[3]);
+/* evolve_gauge_field (field-hmc.h:442-482): U <- exp(i eps P) U with the constraint rules */
+int mag_evolve_gauge(mag_ctx* ctx, double eps);
+/* evolve_momentum (field-hmc.h:427-440) with the force of the current links: P += eps F(U) */
+int mag_evolve_momentum(mag_ctx* ctx, double eps);
+/* reunitarize (field-matrix.h:83-100); maxdev[chain] = max |U' - U| */
+int mag_reunitarize(mag_ctx* ctx, double* maxdev);
+/* stout smearing forward of one chain: level k of the smeared links (k = 0 thin) */
+int mag_stout_level(mag_ctx* ctx, int chain, int level, double* host_aos);
+
+/* ------------------------------------------------------------ integrator */
+/* force_gradient_integrator (field-hmc.h:525-567) or leap_frog_integrator
+   (field-hmc.h:569-587): one molecular-dynamics trajectory, no accept step */
+int mag_integrate(mag_ctx* ctx);
+/* one HMC trajectory of every chain (run_chmc loop body, field-hmc.h:806-843):
+   H_old, integrate, reunitarize, H_new, Metropolis or demon accept, restore on
+   reject.  refresh_momenta = 1 draws momenta from Philox for this trajectory;
+   0 keeps the momenta set by mag_momentum_set.  results[chain] receives the
+   record of each chain (may be NULL). */
+int mag_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results);
+/* n trajectories back to back with Philox momenta, the whole trajectory
+   replayed as one CUDA graph; results[n * n_chains] in trajectory-major order */
+int mag_run(mag_ctx* ctx, int n_traj, mag_traj_result* results);
+/* number of trajectories done so far (the Philox trajectory counter) */
+int mag_traj_counter(mag_ctx* ctx, int64_t* traj);
+int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);
+
+/* ------------------------------------------------------------ measurement */
+/* avg_wilson_loop (field-wloop.h:58-99) for a general spatial vector r and extent T */
+int mag_wilson_loop(mag_ctx* ctx, int chain, const int r[3], int T, double* out);
+/* planar loops R x T for R = 1..Rmax, T = 1..Tmax (r = (R,0,0) and its
+   permutations); out[(R-1) * Tmax + (T-1)] */
+int mag_wilson_loops(mag_ctx* ctx, int chain, int Rmax, int Tmax, double* out);
+/* check_constrained_plaquette (field-matrix.h:407-443) */
+int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAG_C_H */

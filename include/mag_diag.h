@@ -1,0 +1,35 @@
+/*
+ * mag_diag.h -- measurement entry points of libmag_b200.so.
+ *
+ * These have no counterpart in the reference (which only has qlat's TIMER()
+ * scoped timers, field-hmc.h:341 / :903); they exist for benchmarking and
+ * roofline accounting.  All times are CUDA-event times on the context's stream.
+ */
+#ifndef MAG_DIAG_H
+#define MAG_DIAG_H
+
+#include "mag_c.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* device time of the trajectories of the last mag_run call (ms) */
+int mag_last_run_ms(mag_ctx* ctx, double* total_ms);
+/* average device time of one force evaluation (thin or smeared, in the
+   context's precision, constraint fix-up included) on the current links */
+int mag_time_force(mag_ctx* ctx, int reps, double* ms_per_eval);
+/* average device time of one launch of a single kernel on the current
+   fields: "force", "staple", "stout_forward", "stout_lambda", "stout_chain",
+   "evolve", "kick", "action" */
+int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms_per_launch);
+/* number of kernel nodes in the captured trajectory graph (building it if needed) */
+int mag_graph_kernel_count(mag_ctx* ctx, int* kernels);
+/* measured CUDA-core FMA throughput of this device: precision 0 = FP64,
+   1 = FP32; tflops counts 2 flops per FMA */
+int mag_probe_fma_peak(int precision, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MAG_DIAG_H */

@@ -1,0 +1,138 @@
+"""ctypes binding of libmag_b200.so (the C ABI declared in include/mag_c.h).
+
+The library is the only compute path: if it is missing or cannot be loaded
+this module raises, and nothing falls back to a CPU implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmag_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "mag_c.h")
+
+MAG_OK = 0
+MAG_ERR_ARG = -1
+MAG_ERR_CUDA = -2
+MAG_ERR_NAN = -3
+MAG_ERR_STATE = -4
+MAG_ERR_NOMEM = -5
+
+ACTION_WILSON, ACTION_IWASAKI = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+INT_FORCE_GRADIENT, INT_LEAPFROG = 0, 1
+ACCEPT_METROPOLIS, ACCEPT_DEMON = 0, 1
+
+
+class MagParams(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int * 4),
+        ("mag", ctypes.c_int),
+        ("action", ctypes.c_int),
+        ("beta", ctypes.c_double),
+        ("c1", ctypes.c_double),
+        ("rho", ctypes.c_double),
+        ("n_stout", ctypes.c_int),
+        ("tau", ctypes.c_double),
+        ("n_steps", ctypes.c_int),
+        ("precision", ctypes.c_int),
+        ("integrator", ctypes.c_int),
+        ("accept", ctypes.c_int),
+        ("e_max", ctypes.c_double),
+        ("n_forced_accept", ctypes.c_int),
+        ("seed", ctypes.c_uint64),
+    ]
+
+
+class TrajResult(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "h_old", "h_new", "delta_h", "kinetic_old", "kinetic_new", "action_old", "action_new",
+        "plaq_sum_old", "plaq_sum_new", "rect_sum_old", "rect_sum_new", "uniform")] + [
+        ("demon", ctypes.c_double * 2),
+        ("reunit_maxdev", ctypes.c_double),
+        ("avg_plaquette", ctypes.c_double),
+        ("accept", ctypes.c_int),
+        ("traj", ctypes.c_int),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["demon"] = [self.demon[0], self.demon[1]]
+        return d
+
+
+class MagError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where} failed with status {code}: {msg}")
+        self.code = code
+
+
+_DP = ctypes.POINTER(ctypes.c_double)
+_CTX = ctypes.c_void_p
+_IP = ctypes.POINTER(ctypes.c_int)
+
+# name -> argtypes (all return int unless listed in _RESTYPE)
+SIGNATURES = {
+    "mag_ctx_create": [ctypes.POINTER(MagParams), ctypes.POINTER(_CTX)],
+    "mag_ensemble_create": [ctypes.POINTER(MagParams), ctypes.c_int, ctypes.POINTER(_CTX)],
+    "mag_ctx_destroy": [_CTX],
+    "mag_last_error": [],
+    "mag_ctx_num_chains": [_CTX, _IP],
+    "mag_ctx_device_bytes": [_CTX, ctypes.POINTER(ctypes.c_size_t)],
+    "mag_gauge_set": [_CTX, ctypes.c_int, _DP],
+    "mag_gauge_get": [_CTX, ctypes.c_int, _DP],
+    "mag_gauge_hot_start": [_CTX, ctypes.c_uint64],
+    "mag_gauge_cold_start": [_CTX],
+    "mag_momentum_set": [_CTX, ctypes.c_int, _DP],
+    "mag_momentum_get": [_CTX, ctypes.c_int, _DP],
+    "mag_momentum_refresh": [_CTX, ctypes.c_uint64],
+    "mag_uniforms_set": [_CTX, _DP],
+    "mag_gauge_force": [_CTX, ctypes.c_int, _DP],
+    "mag_staple": [_CTX, ctypes.c_int, _DP],
+    "mag_action": [_CTX, ctypes.c_int, _DP, _DP, _DP],
+    "mag_plaquette": [_CTX, ctypes.c_int, _DP],
+    "mag_kinetic": [_CTX, ctypes.c_int, _DP],
+    "mag_hamiltonian": [_CTX, ctypes.c_int, _DP],
+    "mag_evolve_gauge": [_CTX, ctypes.c_double],
+    "mag_evolve_momentum": [_CTX, ctypes.c_double],
+    "mag_reunitarize": [_CTX, _DP],
+    "mag_stout_level": [_CTX, ctypes.c_int, ctypes.c_int, _DP],
+    "mag_integrate": [_CTX],
+    "mag_trajectory": [_CTX, ctypes.c_int, ctypes.POINTER(TrajResult)],
+    "mag_run": [_CTX, ctypes.c_int, ctypes.POINTER(TrajResult)],
+    "mag_traj_counter": [_CTX, ctypes.POINTER(ctypes.c_int64)],
+    "mag_set_traj_counter": [_CTX, ctypes.c_int64],
+    "mag_wilson_loop": [_CTX, ctypes.c_int, _IP, ctypes.c_int, _DP],
+    "mag_wilson_loops": [_CTX, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP],
+    "mag_constrained_plaquette": [_CTX, ctypes.c_int, _DP],
+    "mag_last_run_ms": [_CTX, _DP],
+    "mag_time_force": [_CTX, ctypes.c_int, _DP],
+    "mag_time_kernel": [_CTX, ctypes.c_char_p, ctypes.c_int, _DP],
+    "mag_graph_kernel_count": [_CTX, _IP],
+    "mag_probe_fma_peak": [ctypes.c_int, _DP],
+}
+_RESTYPE = {"mag_last_error": ctypes.c_char_p}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load libmag_b200.so (build it first with ``python -m mag_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m mag_b200.build` (nvcc, sm_100a)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPE.get(name, ctypes.c_int)
+        _lib = lib
+    return _lib
+
+
+def check(code: int, where: str) -> None:
+    if code != MAG_OK:
+        msg = load().mag_last_error()
+        raise MagError(code, where, msg.decode() if msg else "")

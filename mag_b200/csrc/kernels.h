@@ -1,0 +1,135 @@
+// kernels.h -- host-side launchers of the sm_100a kernels (no torch types).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lattice.cuh"
+
+namespace magb {
+
+struct dd2 {
+    double hi, lo;
+};
+
+// Geometry shared by every launch of a context.
+struct DevGeom {
+    const ChainInfo* chains;   // device array [nchain]
+    const uint16_t* c2c;       // device array [vpad / MAG_CHUNK]
+    long vpad;                 // padded global sites (multiple of MAG_CHUNK)
+    int nchain;
+};
+
+// Per-trajectory record kept on the device, one per chain per trajectory.
+struct TrajRecord {
+    double h_old, h_new, delta_h;
+    double kin_old, kin_new, pot_old, pot_new;
+    double plaq_old, plaq_new, rect_old, rect_new;
+    double uniform;
+    double demon0, demon1;
+    double reunit_maxdev;
+    double avg_plaquette;
+    int accept;
+    int traj;
+};
+
+// Device-resident state of the accept step of one chain.
+struct ChainState {
+    double demon0, demon1;
+    int accept;
+    int naccept;
+};
+
+// Slots of the per-chain double-double sums
+enum SumSlot {
+    SLOT_PLAQ_OLD = 0, SLOT_RECT_OLD, SLOT_KIN_OLD,
+    SLOT_PLAQ_NEW, SLOT_RECT_NEW, SLOT_KIN_NEW,
+    SLOT_PLAQ_THIN, SLOT_RECT_THIN, SLOT_SCRATCH,
+    NUM_SLOTS
+};
+
+struct AcceptArgs {
+    int metropolis;          // 1 Metropolis, 0 demon
+    int action_iwasaki;
+    double e_max;
+    int n_forced;
+    const double* uniform_override;  // nullptr: Philox(seed + chain, traj)
+    unsigned long long seed;
+};
+
+// ---- force and staples (kernels_force.cu)
+template <typename T>
+void launch_force(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, bool iwasaki, cudaStream_t s);
+template <typename T>
+void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> Z, bool iwasaki, cudaStream_t s);
+template <typename T>
+void launch_constraint_fixup(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, cudaStream_t s);
+template <typename T>
+void launch_stout_forward(const DevGeom& g, LinkPlanes<T> Uin, LinkPlanes<T> Uout, AlgPlanes<T> Q, cudaStream_t s);
+template <typename T>
+void launch_stout_lambda(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Q, LinkPlanes<T> Z, AlgPlanes<T> Lam,
+                         LinkPlanes<T> Zp, cudaStream_t s);
+template <typename T>
+void launch_stout_chain(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Lam, LinkPlanes<T> Zp, LinkPlanes<T> Zout,
+                        cudaStream_t s);
+template <typename T>
+void launch_stout_chain_force(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Lam, LinkPlanes<T> Zp, AlgPlanes<T> F,
+                              cudaStream_t s);
+
+// ---- streaming kernels (kernels_update.cu)
+template <typename TU, typename TX>
+void launch_evolve(const DevGeom& g, LinkPlanes<TU> Uin, LinkPlanes<TU> Uout, AlgPlanes<TX> X, double eps,
+                   LinkPlanes<float> Ucopy, cudaStream_t s);
+template <typename TF>
+void launch_kick(const DevGeom& g, AlgPlanes<double> P, AlgPlanes<TF> F, double eps, cudaStream_t s);
+// reunit[chain] receives the max deviation as double bits (caller zeroes it first)
+void launch_reunitarize(const DevGeom& g, LinkPlanes<double> U, LinkPlanes<float> Ucopy,
+                        unsigned long long* reunit, cudaStream_t s);
+void launch_copy_to_float(const DevGeom& g, LinkPlanes<double> U, LinkPlanes<float> U32, cudaStream_t s);
+void launch_link_copy(const DevGeom& g, LinkPlanes<double> src, LinkPlanes<double> dst, cudaStream_t s);
+void launch_restore_rejected(const DevGeom& g, LinkPlanes<double> backup, LinkPlanes<double> U,
+                             LinkPlanes<float> U32, const ChainState* st, cudaStream_t s);
+
+// ---- reductions (kernels_update.cu); partial must hold vpad / MAG_CHUNK * 2 dd2
+template <typename T>
+void launch_action_sums(const DevGeom& g, LinkPlanes<T> U, bool with_rect, dd2* partial, dd2* sums, int slot_plaq,
+                        int slot_rect, cudaStream_t s);
+void launch_kinetic_sum(const DevGeom& g, AlgPlanes<double> P, dd2* partial, dd2* sums, int slot, cudaStream_t s);
+void launch_accept(const DevGeom& g, const AcceptArgs& a, dd2* sums, ChainState* st,
+                   const unsigned long long* reunit, TrajRecord* rec, long long* traj_counter, cudaStream_t s);
+// completes rec[] with the thin plaquette, appends it to hist[(counter - *hist_base) * nchain + c]
+// when that index is below hist_cap, then advances the trajectory counter
+void launch_record_plaquette(const DevGeom& g, const dd2* sums, TrajRecord* rec, TrajRecord* hist,
+                             const long long* hist_base, int hist_cap, long long* traj_counter, cudaStream_t s);
+
+// ---- RNG and layout (kernels_update.cu)
+void launch_momenta(const DevGeom& g, AlgPlanes<double> P, unsigned long long seed, const long long* traj_counter,
+                    cudaStream_t s);
+void launch_hot_start(const DevGeom& g, LinkPlanes<double> U, unsigned long long seed, cudaStream_t s);
+void launch_cold_start(const DevGeom& g, LinkPlanes<double> U, cudaStream_t s);
+void launch_aos_to_links(const double* aos, int chain_off, int V, LinkPlanes<double> U, long vpad_unused,
+                         cudaStream_t s);
+void launch_links_to_aos(LinkPlanes<double> U, int chain_off, int V, double* aos, cudaStream_t s);
+template <typename T>
+void launch_aos_to_alg(const double* aos, int chain_off, int V, AlgPlanes<T> X, cudaStream_t s);
+template <typename T>
+void launch_alg_to_aos(AlgPlanes<T> X, int chain_off, int V, double* aos, cudaStream_t s);
+template <typename T>
+void launch_links_to_aos_t(LinkPlanes<T> U, int chain_off, int V, double* aos, cudaStream_t s);
+
+// ---- FMA throughput probe: nblocks x 256 threads, 8 x iters FMAs each
+template <typename T>
+void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s);
+
+// ---- measurements (kernels_wloop.cu)
+// planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;
+// out[((i * Tmax + T-1) * nchain + c) * Rmax + R-1] (i = spatial direction)
+void launch_wilson_planar(const DevGeom& g, LinkPlanes<double> U, int Rmax, int Tmax, LinkPlanes<double> lines,
+                          LinkPlanes<double> tl, LinkPlanes<double> tl2, dd2* partial, dd2* out, cudaStream_t s);
+// sum over sites (coarse sites x = 0 mod coarse_mag when coarse_mag > 0) and
+// npath closed paths of ReTr; dirs[npath][plen], 0..3 forward, 4..7 backward,
+// -1 ends a shorter path; out[c]
+void launch_wilson_general(const DevGeom& g, LinkPlanes<double> U, const int* dirs, int npath, int plen,
+                           int coarse_mag, dd2* partial, dd2* out, cudaStream_t s);
+
+}  // namespace magb

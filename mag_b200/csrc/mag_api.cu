@@ -1,0 +1,1032 @@
+// mag_api.cu -- C++ host driver and C ABI of libmag_b200.so.
+//
+// The context owns every device buffer and one stream.  The integrator is the
+// force-gradient scheme of field-hmc.h:525-567 (or the leapfrog of :569-587)
+// written as a fixed launch sequence with device-resident scalars, so one HMC
+// trajectory (momenta, H_old, integration, reunitarisation, H_new, accept,
+// restore, record) replays as a single CUDA graph with no host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <functional>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mag_c.h"
+#include "../../include/mag_diag.h"
+#include "kernels.h"
+
+using namespace magb;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define MAG_CUDA(call)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (call);                                                                \
+        if (e_ != cudaSuccess)                                                                  \
+            return fail(MAG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+#define MAG_TRY(call)              \
+    do {                           \
+        int r_ = (call);           \
+        if (r_ != MAG_OK) return r_; \
+    } while (0)
+
+constexpr int kHistCap = 256;
+
+template <typename T>
+struct StoutBufs {
+    std::vector<LinkPlanes<T>> lv;   // lv[k] = links after k+1 stout levels
+    std::vector<AlgPlanes<T>> Q;     // Q[k] = exponent of level k -> k+1
+    AlgPlanes<T> lam{nullptr, 0};
+    LinkPlanes<T> za{nullptr, 0}, zp{nullptr, 0};
+};
+
+// host double-double helpers (final action values)
+struct hdd {
+    double hi, lo;
+};
+hdd h_two_sum(double a, double b) {
+    const double s = a + b, bp = s - a;
+    return hdd{s, (a - (s - bp)) + (b - bp)};
+}
+hdd h_add(hdd a, hdd b) {
+    hdd s = h_two_sum(a.hi, b.hi);
+    s.lo += a.lo + b.lo;
+    return h_two_sum(s.hi, s.lo);
+}
+hdd h_mul(hdd a, double b) {
+    const double p = a.hi * b;
+    const double e = std::fma(a.hi, b, -p);
+    return h_two_sum(p, e + a.lo * b);
+}
+hdd h_neg(hdd a) { return hdd{-a.hi, -a.lo}; }
+
+}  // namespace
+
+struct mag_ctx {
+    mag_params p{};
+    std::vector<mag_params> cp;
+    std::vector<ChainInfo> hc;
+    int nchain = 0;
+    long vpad = 0;
+    bool iwasaki = true, mixed = false, any_mag = false;
+    cudaStream_t stream = nullptr;
+    DevGeom geom{};
+    std::vector<void*> allocs;
+    size_t bytes = 0;
+
+    ChainInfo* d_chains = nullptr;
+    uint16_t* d_c2c = nullptr;
+    LinkPlanes<double> U{nullptr, 0}, Ubak{nullptr, 0}, Uaux{nullptr, 0};
+    AlgPlanes<double> P{nullptr, 0}, F{nullptr, 0};
+    LinkPlanes<float> U32{nullptr, 0}, Uaux32{nullptr, 0};
+    AlgPlanes<float> F32{nullptr, 0};
+    StoutBufs<double> st64;
+    StoutBufs<float> st32;
+    dd2* partial = nullptr;
+    dd2* sums = nullptr;
+    ChainState* cstate = nullptr;
+    unsigned long long* reunit = nullptr;
+    TrajRecord* rec = nullptr;
+    TrajRecord* hist = nullptr;
+    long long* hist_base = nullptr;
+    long long* traj_counter = nullptr;
+    long long* tmp_counter = nullptr;
+    double* d_uniform = nullptr;
+    bool uniform_override = false;
+    double* staging = nullptr;
+    long max_v = 0;
+    long long host_traj = 0;
+    cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_run_ms = 0.0;
+
+    ~mag_ctx() { release(); }
+
+    void release() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        for (void* a : allocs) cudaFree(a);
+        allocs.clear();
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        ev0 = ev1 = nullptr;
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+
+    int alloc(void** ptr, size_t n) {
+        cudaError_t e = cudaMalloc(ptr, n);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(MAG_ERR_NOMEM, "cudaMalloc(" + std::to_string(n) + " bytes): " + cudaGetErrorString(e));
+        }
+        allocs.push_back(*ptr);
+        bytes += n;
+        return MAG_OK;
+    }
+    template <typename T>
+    int alloc_links(LinkPlanes<T>& l) {
+        l.vpad = vpad;
+        return alloc((void**)&l.p, sizeof(cplx<T>) * 36 * (size_t)vpad);
+    }
+    template <typename T>
+    int alloc_alg(AlgPlanes<T>& a) {
+        a.vpad = vpad;
+        return alloc((void**)&a.p, sizeof(T) * 32 * (size_t)vpad);
+    }
+    template <typename T>
+    int alloc_stout(StoutBufs<T>& b, bool backward) {
+        b.lv.resize(p.n_stout);
+        b.Q.resize(p.n_stout);
+        for (int k = 0; k < p.n_stout; k++) {
+            MAG_TRY(alloc_links(b.lv[k]));
+            MAG_TRY(alloc_alg(b.Q[k]));
+        }
+        if (backward && p.n_stout > 0) {
+            MAG_TRY(alloc_alg(b.lam));
+            MAG_TRY(alloc_links(b.za));
+            MAG_TRY(alloc_links(b.zp));
+        }
+        return MAG_OK;
+    }
+
+    int check(const char* what) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(MAG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        return MAG_OK;
+    }
+    int sync(const char* what) {
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return fail(MAG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        return check(what);
+    }
+
+    int init(const mag_params* params, int n) {
+        p = params[0];
+        nchain = n;
+        iwasaki = p.action == MAG_ACTION_IWASAKI;
+        mixed = p.precision == MAG_PREC_MIXED;
+        long off = 0;
+        for (int c = 0; c < n; c++) {
+            const mag_params& q = params[c];
+            ChainInfo ci{};
+            long V = 1;
+            for (int d = 0; d < 4; d++) {
+                if (q.dims[d] < 2) return fail(MAG_ERR_ARG, "every lattice extent must be >= 2");
+                if (q.mag < 0 || (q.mag > 0 && q.dims[d] % q.mag != 0))
+                    return fail(MAG_ERR_ARG, "lattice extents must be divisible by mag");
+                ci.L[d] = q.dims[d];
+                ci.stride[d] = (int)V;
+                V *= q.dims[d];
+            }
+            if (q.mag == 1) return fail(MAG_ERR_ARG, "mag = 1 freezes every link (field-hmc.h:331); use 0 or >= 2");
+            if (q.action != p.action) return fail(MAG_ERR_ARG, "all chains of an ensemble share the action type");
+            ci.V = (int)V;
+            ci.off = (int)off;
+            ci.mag = q.mag;
+            ci.beta = q.beta;
+            ci.c1 = iwasaki ? q.c1 : 0.0;
+            ci.c0 = 1.0 - 8.0 * ci.c1;
+            ci.rho = q.rho;
+            hc.push_back(ci);
+            cp.push_back(q);
+            any_mag = any_mag || q.mag > 0;
+            max_v = std::max(max_v, V);
+            off += (V + MAG_CHUNK - 1) / MAG_CHUNK * MAG_CHUNK;
+        }
+        if (off >= (1L << 31) / 36) return fail(MAG_ERR_ARG, "total volume too large for 32-bit site indices");
+        if (p.n_steps < 1 || p.n_stout < 0 || p.n_stout > 8) return fail(MAG_ERR_ARG, "bad n_steps or n_stout");
+        vpad = off;
+        MAG_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        MAG_CUDA(cudaEventCreate(&ev0));
+        MAG_CUDA(cudaEventCreate(&ev1));
+        MAG_TRY(alloc((void**)&d_chains, sizeof(ChainInfo) * n));
+        const long nchunk = vpad / MAG_CHUNK;
+        MAG_TRY(alloc((void**)&d_c2c, sizeof(uint16_t) * nchunk));
+        std::vector<uint16_t> c2c(nchunk, 0);
+        for (int c = 0; c < n; c++)
+            for (long k = hc[c].off / MAG_CHUNK; k < (hc[c].off + hc[c].V + MAG_CHUNK - 1) / MAG_CHUNK; k++)
+                c2c[k] = (uint16_t)c;
+        MAG_CUDA(cudaMemcpy(d_chains, hc.data(), sizeof(ChainInfo) * n, cudaMemcpyHostToDevice));
+        MAG_CUDA(cudaMemcpy(d_c2c, c2c.data(), sizeof(uint16_t) * nchunk, cudaMemcpyHostToDevice));
+        geom = DevGeom{d_chains, d_c2c, vpad, n};
+
+        MAG_TRY(alloc_links(U));
+        MAG_TRY(alloc_links(Ubak));
+        MAG_TRY(alloc_alg(P));
+        if (mixed) {
+            MAG_TRY(alloc_links(U32));
+            MAG_TRY(alloc_links(Uaux32));
+            MAG_TRY(alloc_alg(F32));
+            MAG_TRY(alloc_stout(st32, true));
+            MAG_TRY(alloc_stout(st64, false));  // FP64 forward smearing for the Hamiltonian
+            MAG_TRY(alloc_alg(F));              // FP64 force for single-call API use
+        } else {
+            MAG_TRY(alloc_links(Uaux));
+            MAG_TRY(alloc_alg(F));
+            MAG_TRY(alloc_stout(st64, true));
+        }
+        MAG_TRY(alloc((void**)&partial, sizeof(dd2) * 2 * (nchunk + 1)));
+        MAG_TRY(alloc((void**)&sums, sizeof(dd2) * NUM_SLOTS * n));
+        MAG_TRY(alloc((void**)&cstate, sizeof(ChainState) * n));
+        MAG_TRY(alloc((void**)&reunit, sizeof(unsigned long long) * n));
+        MAG_TRY(alloc((void**)&rec, sizeof(TrajRecord) * n));
+        MAG_TRY(alloc((void**)&hist, sizeof(TrajRecord) * n * kHistCap));
+        MAG_TRY(alloc((void**)&hist_base, sizeof(long long)));
+        MAG_TRY(alloc((void**)&traj_counter, sizeof(long long)));
+        MAG_TRY(alloc((void**)&tmp_counter, sizeof(long long)));
+        MAG_TRY(alloc((void**)&d_uniform, sizeof(double) * n));
+        MAG_TRY(alloc((void**)&staging, sizeof(double) * 72 * (size_t)max_v));
+        MAG_CUDA(cudaMemsetAsync(cstate, 0, sizeof(ChainState) * n, stream));
+        MAG_CUDA(cudaMemsetAsync(reunit, 0, sizeof(unsigned long long) * n, stream));
+        MAG_CUDA(cudaMemsetAsync(traj_counter, 0, sizeof(long long), stream));
+        MAG_CUDA(cudaMemsetAsync(hist_base, 0, sizeof(long long), stream));
+        launch_cold_start(geom, U, stream);
+        MAG_TRY(refresh_copy());
+        return sync("context init");
+    }
+
+    int refresh_copy() {
+        if (mixed) launch_copy_to_float(geom, U, U32, stream);
+        return check("refresh fp32 links");
+    }
+
+    // ----------------------------------------------------------- force
+    template <typename T>
+    void force_eval(LinkPlanes<T> Uin, AlgPlanes<T> Fout, StoutBufs<T>& b) {
+        if (p.n_stout == 0) {
+            launch_force<T>(geom, Uin, Fout, iwasaki, stream);
+        } else {
+            LinkPlanes<T> cur = Uin;
+            for (int k = 0; k < p.n_stout; k++) {
+                launch_stout_forward<T>(geom, cur, b.lv[k], b.Q[k], stream);
+                cur = b.lv[k];
+            }
+            launch_staple_dagger<T>(geom, cur, b.za, iwasaki, stream);
+            for (int k = p.n_stout - 1; k >= 0; k--) {
+                LinkPlanes<T> ul = k == 0 ? Uin : b.lv[k - 1];
+                launch_stout_lambda<T>(geom, ul, b.Q[k], b.za, b.lam, b.zp, stream);
+                if (k == 0) launch_stout_chain_force<T>(geom, ul, b.lam, b.zp, Fout, stream);
+                else launch_stout_chain<T>(geom, ul, b.lam, b.zp, b.za, stream);
+            }
+        }
+        if (any_mag) launch_constraint_fixup<T>(geom, Uin, Fout, stream);
+    }
+
+    // smeared FP64 links for the Hamiltonian (the thin links when n_stout = 0)
+    LinkPlanes<double> smear64() {
+        LinkPlanes<double> cur = U;
+        for (int k = 0; k < p.n_stout; k++) {
+            launch_stout_forward<double>(geom, cur, st64.lv[k], st64.Q[k], stream);
+            cur = st64.lv[k];
+        }
+        return cur;
+    }
+
+    void hamiltonian_sums(bool is_new) {
+        launch_kinetic_sum(geom, P, partial, sums, is_new ? SLOT_KIN_NEW : SLOT_KIN_OLD, stream);
+        LinkPlanes<double> top = smear64();
+        launch_action_sums<double>(geom, top, true, partial, sums, is_new ? SLOT_PLAQ_NEW : SLOT_PLAQ_OLD,
+                                   is_new ? SLOT_RECT_NEW : SLOT_RECT_OLD, stream);
+    }
+
+    // ------------------------------------------------------- integrator
+    template <typename T>
+    void integrate_t(LinkPlanes<T> Ut, LinkPlanes<T> Ua, AlgPlanes<T> Fw, StoutBufs<T>& b) {
+        const double dt = p.tau / p.n_steps;
+        LinkPlanes<float> copy = mixed ? U32 : LinkPlanes<float>{nullptr, 0};
+        auto master = [&](double eps) { launch_evolve<double, double>(geom, U, U, P, eps, copy, stream); };
+        if (p.integrator == MAG_INT_LEAPFROG) {
+            master(dt / 2.);
+            for (int i = 0; i < p.n_steps; i++) {
+                force_eval<T>(Ut, Fw, b);
+                launch_kick<T>(geom, P, Fw, dt, stream);
+                master(i < p.n_steps - 1 ? dt : dt / 2.);
+            }
+            return;
+        }
+        const double alpha = (3. - std::sqrt(3.)) * dt / 6.;
+        const double beta = dt / std::sqrt(3.);
+        const double gamma = (2. - std::sqrt(3.)) * dt * dt / 12.;
+        auto fg_kick = [&]() {
+            force_eval<T>(Ut, Fw, b);
+            launch_evolve<T, T>(geom, Ut, Ua, Fw, gamma, LinkPlanes<float>{nullptr, 0}, stream);
+            force_eval<T>(Ua, Fw, b);
+            launch_kick<T>(geom, P, Fw, 0.5 * dt, stream);
+        };
+        master(alpha);
+        for (int i = 0; i < p.n_steps; i++) {
+            fg_kick();
+            master(beta);
+            fg_kick();
+            master(i < p.n_steps - 1 ? 2. * alpha : alpha);
+        }
+    }
+
+    int integrate() {
+        if (mixed) integrate_t<float>(U32, Uaux32, F32, st32);
+        else integrate_t<double>(U, Uaux, F, st64);
+        cudaMemsetAsync(reunit, 0, sizeof(unsigned long long) * nchain, stream);
+        if (p.integrator != MAG_INT_LEAPFROG)
+            launch_reunitarize(geom, U, mixed ? U32 : LinkPlanes<float>{nullptr, 0}, reunit, stream);
+        return check("integrate");
+    }
+
+    // one trajectory as a fixed launch sequence
+    int trajectory_body(bool refresh) {
+        if (refresh) launch_momenta(geom, P, p.seed, traj_counter, stream);
+        launch_link_copy(geom, U, Ubak, stream);
+        hamiltonian_sums(false);
+        MAG_TRY(integrate());
+        hamiltonian_sums(true);
+        AcceptArgs a;
+        a.metropolis = p.accept == MAG_ACCEPT_METROPOLIS ? 1 : 0;
+        a.action_iwasaki = iwasaki ? 1 : 0;
+        a.e_max = p.e_max;
+        a.n_forced = p.n_forced_accept;
+        a.uniform_override = uniform_override ? d_uniform : nullptr;
+        a.seed = p.seed;
+        launch_accept(geom, a, sums, cstate, reunit, rec, traj_counter, stream);
+        launch_restore_rejected(geom, Ubak, U, mixed ? U32 : LinkPlanes<float>{nullptr, 0}, cstate, stream);
+        launch_action_sums<double>(geom, U, false, partial, sums, SLOT_PLAQ_THIN, SLOT_RECT_THIN, stream);
+        launch_record_plaquette(geom, sums, rec, hist, hist_base, kHistCap, traj_counter, stream);
+        return check("trajectory");
+    }
+
+    int build_graph() {
+        if (graph) return MAG_OK;
+        cudaGraph_t g;
+        MAG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        int r = trajectory_body(true);
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        if (r != MAG_OK) return r;
+        if (e != cudaSuccess) return fail(MAG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        std::vector<cudaGraphNode_t> nodes(nn);
+        cudaGraphGetNodes(g, nodes.data(), &nn);
+        graph_kernels = 0;
+        for (size_t k = 0; k < nn; k++) {
+            cudaGraphNodeType t;
+            cudaGraphNodeGetType(nodes[k], &t);
+            if (t == cudaGraphNodeTypeKernel) graph_kernels++;
+        }
+        e = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(MAG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        return MAG_OK;
+    }
+
+    static void to_result(const TrajRecord& r, mag_traj_result* o) {
+        o->h_old = r.h_old; o->h_new = r.h_new; o->delta_h = r.delta_h;
+        o->kinetic_old = r.kin_old; o->kinetic_new = r.kin_new;
+        o->action_old = r.pot_old; o->action_new = r.pot_new;
+        o->plaq_sum_old = r.plaq_old; o->plaq_sum_new = r.plaq_new;
+        o->rect_sum_old = r.rect_old; o->rect_sum_new = r.rect_new;
+        o->uniform = r.uniform;
+        o->demon[0] = r.demon0; o->demon[1] = r.demon1;
+        o->reunit_maxdev = r.reunit_maxdev;
+        o->avg_plaquette = r.avg_plaquette;
+        o->accept = r.accept;
+        o->traj = r.traj;
+    }
+
+    // lazily sized measurement buffers (Wilson loops, closed paths)
+    dd2* wl_partial = nullptr;
+    dd2* wl_out = nullptr;
+    cplx<double>* wl_lines = nullptr;
+    int* d_paths = nullptr;
+    int wl_rmax = 0, wl_tmax = 0;
+    const int max_path_ints = 4096;
+
+    void free_one(void* p) {
+        if (!p) return;
+        for (size_t k = 0; k < allocs.size(); k++)
+            if (allocs[k] == p) {
+                allocs.erase(allocs.begin() + k);
+                break;
+            }
+        cudaFree(p);
+    }
+
+    // Rmax x Tmax planar loops need Rmax + 2 single-direction line planes
+    int ensure_meas(int Rmax, int Tmax, bool lines) {
+        if (!d_paths) MAG_TRY(alloc((void**)&d_paths, sizeof(int) * max_path_ints));
+        const bool grow = !wl_partial || Rmax > wl_rmax || Tmax > wl_tmax || (lines && !wl_lines);
+        if (!grow) return MAG_OK;
+        cudaStreamSynchronize(stream);
+        Rmax = std::max(Rmax, wl_rmax);
+        Tmax = std::max(Tmax, wl_tmax);
+        const size_t nb = (size_t)(vpad / MAG_CHUNK) + 1;
+        free_one(wl_partial);
+        free_one(wl_out);
+        free_one(wl_lines);
+        wl_lines = nullptr;
+        MAG_TRY(alloc((void**)&wl_partial, sizeof(dd2) * nb * Rmax));
+        MAG_TRY(alloc((void**)&wl_out, sizeof(dd2) * ((size_t)3 * Tmax * nchain * Rmax + nchain)));
+        if (lines) MAG_TRY(alloc((void**)&wl_lines, sizeof(cplx<double>) * 9 * (size_t)vpad * (Rmax + 2)));
+        wl_rmax = Rmax;
+        wl_tmax = Tmax;
+        return MAG_OK;
+    }
+
+    int chain_ok(int c) {
+        if (c < 0 || c >= nchain) return fail(MAG_ERR_ARG, "chain index out of range");
+        return MAG_OK;
+    }
+
+    // read per-chain double-double sums back to the host
+    int read_sums(std::vector<dd2>& out) {
+        out.resize((size_t)NUM_SLOTS * nchain);
+        MAG_CUDA(cudaMemcpyAsync(out.data(), sums, sizeof(dd2) * out.size(), cudaMemcpyDeviceToHost, stream));
+        return sync("read sums");
+    }
+
+    hdd action_value(int c, dd2 plaq, dd2 rect) const {
+        const ChainInfo& ci = hc[c];
+        hdd t = iwasaki ? h_add(h_mul(h_neg(hdd{plaq.hi, plaq.lo}), ci.c0), h_mul(h_neg(hdd{rect.hi, rect.lo}), ci.c1))
+                        : h_neg(hdd{plaq.hi, plaq.lo});
+        return h_mul(t, ci.beta / 3.0);
+    }
+};
+
+// ======================================================================= C ABI
+extern "C" {
+
+const char* mag_last_error(void) { return g_last_error.c_str(); }
+
+int mag_ensemble_create(const mag_params* p, int n, mag_ctx** out) {
+    if (!p || !out || n < 1 || n > 1024) return fail(MAG_ERR_ARG, "mag_ensemble_create: bad arguments");
+    *out = nullptr;
+    mag_ctx* c = new mag_ctx();
+    const int r = c->init(p, n);
+    if (r != MAG_OK) {
+        delete c;
+        return r;
+    }
+    *out = c;
+    return MAG_OK;
+}
+
+int mag_ctx_create(const mag_params* p, mag_ctx** out) { return mag_ensemble_create(p, 1, out); }
+
+int mag_ctx_destroy(mag_ctx* ctx) {
+    if (!ctx) return MAG_ERR_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+    return MAG_OK;
+}
+
+int mag_ctx_num_chains(const mag_ctx* ctx, int* n) {
+    if (!ctx || !n) return MAG_ERR_ARG;
+    *n = ctx->nchain;
+    return MAG_OK;
+}
+
+int mag_ctx_device_bytes(const mag_ctx* ctx, size_t* bytes) {
+    if (!ctx || !bytes) return MAG_ERR_ARG;
+    *bytes = ctx->bytes;
+    return MAG_OK;
+}
+
+int mag_gauge_set(mag_ctx* ctx, int chain, const double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_gauge_set: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    MAG_CUDA(cudaMemcpyAsync(ctx->staging, host, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    launch_aos_to_links(ctx->staging, ci.off, ci.V, ctx->U, ctx->vpad, ctx->stream);
+    MAG_TRY(ctx->refresh_copy());
+    return ctx->sync("mag_gauge_set");
+}
+
+int mag_gauge_get(mag_ctx* ctx, int chain, double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_gauge_get: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    launch_links_to_aos(ctx->U, ci.off, ci.V, ctx->staging, ctx->stream);
+    MAG_CUDA(cudaMemcpyAsync(host, ctx->staging, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return ctx->sync("mag_gauge_get");
+}
+
+int mag_gauge_hot_start(mag_ctx* ctx, uint64_t seed) {
+    if (!ctx) return MAG_ERR_ARG;
+    launch_hot_start(ctx->geom, ctx->U, seed, ctx->stream);
+    MAG_TRY(ctx->refresh_copy());
+    return ctx->sync("mag_gauge_hot_start");
+}
+
+int mag_gauge_cold_start(mag_ctx* ctx) {
+    if (!ctx) return MAG_ERR_ARG;
+    launch_cold_start(ctx->geom, ctx->U, ctx->stream);
+    MAG_TRY(ctx->refresh_copy());
+    return ctx->sync("mag_gauge_cold_start");
+}
+
+int mag_momentum_set(mag_ctx* ctx, int chain, const double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_momentum_set: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    MAG_CUDA(cudaMemcpyAsync(ctx->staging, host, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    launch_aos_to_alg<double>(ctx->staging, ci.off, ci.V, ctx->P, ctx->stream);
+    return ctx->sync("mag_momentum_set");
+}
+
+int mag_momentum_get(mag_ctx* ctx, int chain, double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_momentum_get: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    launch_alg_to_aos<double>(ctx->P, ci.off, ci.V, ctx->staging, ctx->stream);
+    MAG_CUDA(cudaMemcpyAsync(host, ctx->staging, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return ctx->sync("mag_momentum_get");
+}
+
+int mag_momentum_refresh(mag_ctx* ctx, uint64_t traj) {
+    if (!ctx) return MAG_ERR_ARG;
+    const long long t = (long long)traj;
+    MAG_CUDA(cudaMemcpyAsync(ctx->tmp_counter, &t, sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    launch_momenta(ctx->geom, ctx->P, ctx->p.seed, ctx->tmp_counter, ctx->stream);
+    return ctx->sync("mag_momentum_refresh");
+}
+
+int mag_uniforms_set(mag_ctx* ctx, const double* u) {
+    if (!ctx) return MAG_ERR_ARG;
+    const bool was = ctx->uniform_override;
+    if (!u) {
+        ctx->uniform_override = false;
+    } else {
+        MAG_CUDA(cudaMemcpyAsync(ctx->d_uniform, u, sizeof(double) * ctx->nchain, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        ctx->uniform_override = true;
+    }
+    if (was != ctx->uniform_override && ctx->graph) {
+        cudaGraphExecDestroy(ctx->graph);
+        ctx->graph = nullptr;
+    }
+    return ctx->sync("mag_uniforms_set");
+}
+
+int mag_gauge_force(mag_ctx* ctx, int chain, double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_gauge_force: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    if (ctx->mixed) {
+        ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
+        launch_alg_to_aos<float>(ctx->F32, ci.off, ci.V, ctx->staging, ctx->stream);
+    } else {
+        ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
+        launch_alg_to_aos<double>(ctx->F, ci.off, ci.V, ctx->staging, ctx->stream);
+    }
+    MAG_TRY(ctx->check("mag_gauge_force"));
+    MAG_CUDA(cudaMemcpyAsync(host, ctx->staging, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return ctx->sync("mag_gauge_force");
+}
+
+int mag_staple(mag_ctx* ctx, int chain, double* host) {
+    if (!ctx || !host) return fail(MAG_ERR_ARG, "mag_staple: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    if (ctx->mixed) {
+        LinkPlanes<float> cur = ctx->U32;
+        for (int k = 0; k < ctx->p.n_stout; k++) {
+            launch_stout_forward<float>(ctx->geom, cur, ctx->st32.lv[k], ctx->st32.Q[k], ctx->stream);
+            cur = ctx->st32.lv[k];
+        }
+        LinkPlanes<float> z = ctx->p.n_stout ? ctx->st32.za : ctx->Uaux32;
+        launch_staple_dagger<float>(ctx->geom, cur, z, ctx->iwasaki, ctx->stream);
+        launch_links_to_aos_t<float>(z, ci.off, ci.V, ctx->staging, ctx->stream);
+    } else {
+        LinkPlanes<double> cur = ctx->smear64();
+        LinkPlanes<double> z = ctx->p.n_stout ? ctx->st64.za : ctx->Uaux;
+        launch_staple_dagger<double>(ctx->geom, cur, z, ctx->iwasaki, ctx->stream);
+        launch_links_to_aos_t<double>(z, ci.off, ci.V, ctx->staging, ctx->stream);
+    }
+    MAG_TRY(ctx->check("mag_staple"));
+    MAG_CUDA(cudaMemcpyAsync(host, ctx->staging, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return ctx->sync("mag_staple");
+}
+
+int mag_action(mag_ctx* ctx, int chain, double* plaq, double* rect, double* action) {
+    if (!ctx) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    LinkPlanes<double> top = ctx->smear64();
+    launch_action_sums<double>(ctx->geom, top, true, ctx->partial, ctx->sums, SLOT_PLAQ_THIN, SLOT_RECT_THIN,
+                               ctx->stream);
+    MAG_TRY(ctx->check("mag_action"));
+    std::vector<dd2> s;
+    MAG_TRY(ctx->read_sums(s));
+    const dd2 pl = s[chain * NUM_SLOTS + SLOT_PLAQ_THIN], re = s[chain * NUM_SLOTS + SLOT_RECT_THIN];
+    if (plaq) *plaq = pl.hi + pl.lo;
+    if (rect) *rect = re.hi + re.lo;
+    const hdd a = ctx->action_value(chain, pl, re);
+    if (action) *action = a.hi + a.lo;
+    return MAG_OK;
+}
+
+int mag_plaquette(mag_ctx* ctx, int chain, double* avg) {
+    if (!ctx || !avg) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    launch_action_sums<double>(ctx->geom, ctx->U, false, ctx->partial, ctx->sums, SLOT_SCRATCH, SLOT_SCRATCH,
+                               ctx->stream);
+    MAG_TRY(ctx->check("mag_plaquette"));
+    std::vector<dd2> s;
+    MAG_TRY(ctx->read_sums(s));
+    const dd2 pl = s[chain * NUM_SLOTS + SLOT_SCRATCH];
+    *avg = (pl.hi + pl.lo) / (18.0 * ctx->hc[chain].V);
+    return MAG_OK;
+}
+
+int mag_kinetic(mag_ctx* ctx, int chain, double* kin) {
+    if (!ctx || !kin) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    launch_kinetic_sum(ctx->geom, ctx->P, ctx->partial, ctx->sums, SLOT_SCRATCH, ctx->stream);
+    MAG_TRY(ctx->check("mag_kinetic"));
+    std::vector<dd2> s;
+    MAG_TRY(ctx->read_sums(s));
+    const dd2 k = s[chain * NUM_SLOTS + SLOT_SCRATCH];
+    *kin = k.hi + k.lo;
+    return MAG_OK;
+}
+
+int mag_hamiltonian(mag_ctx* ctx, int chain, double out[3]) {
+    if (!ctx || !out) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    ctx->hamiltonian_sums(false);
+    MAG_TRY(ctx->check("mag_hamiltonian"));
+    std::vector<dd2> s;
+    MAG_TRY(ctx->read_sums(s));
+    const dd2* S = s.data() + chain * NUM_SLOTS;
+    const hdd a = ctx->action_value(chain, S[SLOT_PLAQ_OLD], S[SLOT_RECT_OLD]);
+    const hdd k = hdd{S[SLOT_KIN_OLD].hi, S[SLOT_KIN_OLD].lo};
+    const hdd h = h_add(a, k);
+    out[0] = h.hi + h.lo;
+    out[1] = k.hi + k.lo;
+    out[2] = a.hi + a.lo;
+    return MAG_OK;
+}
+
+int mag_evolve_gauge(mag_ctx* ctx, double eps) {
+    if (!ctx) return MAG_ERR_ARG;
+    launch_evolve<double, double>(ctx->geom, ctx->U, ctx->U, ctx->P, eps,
+                                  ctx->mixed ? ctx->U32 : LinkPlanes<float>{nullptr, 0}, ctx->stream);
+    return ctx->sync("mag_evolve_gauge");
+}
+
+int mag_evolve_momentum(mag_ctx* ctx, double eps) {
+    if (!ctx) return MAG_ERR_ARG;
+    if (ctx->mixed) {
+        ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
+        launch_kick<float>(ctx->geom, ctx->P, ctx->F32, eps, ctx->stream);
+    } else {
+        ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
+        launch_kick<double>(ctx->geom, ctx->P, ctx->F, eps, ctx->stream);
+    }
+    return ctx->sync("mag_evolve_momentum");
+}
+
+int mag_reunitarize(mag_ctx* ctx, double* maxdev) {
+    if (!ctx) return MAG_ERR_ARG;
+    MAG_CUDA(cudaMemsetAsync(ctx->reunit, 0, sizeof(unsigned long long) * ctx->nchain, ctx->stream));
+    launch_reunitarize(ctx->geom, ctx->U, ctx->mixed ? ctx->U32 : LinkPlanes<float>{nullptr, 0}, ctx->reunit,
+                       ctx->stream);
+    MAG_TRY(ctx->check("mag_reunitarize"));
+    std::vector<unsigned long long> bits(ctx->nchain);
+    MAG_CUDA(cudaMemcpyAsync(bits.data(), ctx->reunit, sizeof(unsigned long long) * ctx->nchain,
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    MAG_TRY(ctx->sync("mag_reunitarize"));
+    if (maxdev)
+        for (int c = 0; c < ctx->nchain; c++) std::memcpy(&maxdev[c], &bits[c], sizeof(double));
+    return MAG_OK;
+}
+
+int mag_stout_level(mag_ctx* ctx, int chain, int level, double* host) {
+    if (!ctx || !host) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    if (level < 0 || level > ctx->p.n_stout) return fail(MAG_ERR_ARG, "stout level out of range");
+    const ChainInfo& ci = ctx->hc[chain];
+    ctx->smear64();
+    LinkPlanes<double> l = level == 0 ? ctx->U : ctx->st64.lv[level - 1];
+    launch_links_to_aos(l, ci.off, ci.V, ctx->staging, ctx->stream);
+    MAG_TRY(ctx->check("mag_stout_level"));
+    MAG_CUDA(cudaMemcpyAsync(host, ctx->staging, sizeof(double) * 72 * (size_t)ci.V, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    return ctx->sync("mag_stout_level");
+}
+
+int mag_integrate(mag_ctx* ctx) {
+    if (!ctx) return MAG_ERR_ARG;
+    MAG_TRY(ctx->integrate());
+    return ctx->sync("mag_integrate");
+}
+
+int mag_trajectory(mag_ctx* ctx, int refresh, mag_traj_result* results) {
+    if (!ctx) return MAG_ERR_ARG;
+    MAG_TRY(ctx->trajectory_body(refresh != 0));
+    std::vector<TrajRecord> r(ctx->nchain);
+    MAG_CUDA(cudaMemcpyAsync(r.data(), ctx->rec, sizeof(TrajRecord) * ctx->nchain, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    MAG_TRY(ctx->sync("mag_trajectory"));
+    ctx->host_traj++;
+    bool finite = true;
+    for (int c = 0; c < ctx->nchain; c++) {
+        if (results) mag_ctx::to_result(r[c], &results[c]);
+        finite = finite && std::isfinite(r[c].delta_h);
+    }
+    if (!finite) return fail(MAG_ERR_NAN, "non-finite Delta H");
+    return MAG_OK;
+}
+
+int mag_run(mag_ctx* ctx, int n_traj, mag_traj_result* results) {
+    if (!ctx || n_traj < 0) return MAG_ERR_ARG;
+    MAG_TRY(ctx->build_graph());
+    std::vector<TrajRecord> r;
+    double total = 0.0;
+    bool finite = true;
+    for (int done = 0; done < n_traj;) {
+        const int chunk = std::min(kHistCap, n_traj - done);
+        const long long base = ctx->host_traj;
+        MAG_CUDA(cudaMemcpyAsync(ctx->hist_base, &base, sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+        MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+        for (int i = 0; i < chunk; i++) MAG_CUDA(cudaGraphLaunch(ctx->graph, ctx->stream));
+        MAG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+        r.resize((size_t)chunk * ctx->nchain);
+        MAG_CUDA(cudaMemcpyAsync(r.data(), ctx->hist, sizeof(TrajRecord) * r.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        MAG_TRY(ctx->sync("mag_run"));
+        float ms = 0.f;
+        MAG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+        total += ms;
+        for (size_t k = 0; k < r.size(); k++) {
+            if (results) mag_ctx::to_result(r[k], &results[(size_t)done * ctx->nchain + k]);
+            finite = finite && std::isfinite(r[k].delta_h);
+        }
+        ctx->host_traj += chunk;
+        done += chunk;
+    }
+    ctx->last_run_ms = total;
+    if (!finite) return fail(MAG_ERR_NAN, "non-finite Delta H");
+    return MAG_OK;
+}
+
+int mag_traj_counter(mag_ctx* ctx, int64_t* traj) {
+    if (!ctx || !traj) return MAG_ERR_ARG;
+    *traj = ctx->host_traj;
+    return MAG_OK;
+}
+
+int mag_set_traj_counter(mag_ctx* ctx, int64_t traj) {
+    if (!ctx || traj < 0) return MAG_ERR_ARG;
+    const long long t = traj;
+    MAG_CUDA(cudaMemcpyAsync(ctx->traj_counter, &t, sizeof(long long), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->host_traj = traj;
+    return ctx->sync("mag_set_traj_counter");
+}
+
+int mag_last_run_ms(mag_ctx* ctx, double* total_ms) {
+    if (!ctx || !total_ms) return MAG_ERR_ARG;
+    *total_ms = ctx->last_run_ms;
+    return MAG_OK;
+}
+
+int mag_time_force(mag_ctx* ctx, int reps, double* ms) {
+    if (!ctx || !ms || reps < 1) return MAG_ERR_ARG;
+    auto once = [&]() {
+        if (ctx->mixed) ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
+        else ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
+    };
+    once();
+    MAG_TRY(ctx->sync("mag_time_force warm-up"));
+    MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (int i = 0; i < reps; i++) once();
+    MAG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    MAG_TRY(ctx->sync("mag_time_force"));
+    float t = 0.f;
+    MAG_CUDA(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    *ms = t / reps;
+    return MAG_OK;
+}
+
+int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms) {
+    if (!ctx || !which || !ms || reps < 1) return MAG_ERR_ARG;
+    const std::string w(which);
+    std::function<void()> f;
+    const bool m = ctx->mixed;
+    const int L = ctx->p.n_stout;
+    auto& g = ctx->geom;
+    cudaStream_t s = ctx->stream;
+    if ((w == "stout_forward" || w == "stout_lambda" || w == "stout_chain") && L == 0)
+        return fail(MAG_ERR_STATE, "mag_time_kernel: no stout levels in this context");
+    // one full force evaluation first, so every intermediate buffer holds live data
+    if (m) ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
+    else ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
+    if (w == "force") {
+        f = [&]() {
+            if (m) launch_force<float>(g, ctx->U32, ctx->F32, ctx->iwasaki, s);
+            else launch_force<double>(g, ctx->U, ctx->F, ctx->iwasaki, s);
+        };
+    } else if (w == "staple") {
+        f = [&]() {
+            if (m) launch_staple_dagger<float>(g, L ? ctx->st32.lv[L - 1] : ctx->U32, L ? ctx->st32.za : ctx->Uaux32,
+                                               ctx->iwasaki, s);
+            else launch_staple_dagger<double>(g, L ? ctx->st64.lv[L - 1] : ctx->U, L ? ctx->st64.za : ctx->Uaux,
+                                              ctx->iwasaki, s);
+        };
+    } else if (w == "stout_forward") {
+        f = [&]() {
+            if (m) launch_stout_forward<float>(g, ctx->U32, ctx->st32.lv[0], ctx->st32.Q[0], s);
+            else launch_stout_forward<double>(g, ctx->U, ctx->st64.lv[0], ctx->st64.Q[0], s);
+        };
+    } else if (w == "stout_lambda") {
+        f = [&]() {
+            if (m) launch_stout_lambda<float>(g, ctx->U32, ctx->st32.Q[0], ctx->st32.za, ctx->st32.lam, ctx->st32.zp, s);
+            else launch_stout_lambda<double>(g, ctx->U, ctx->st64.Q[0], ctx->st64.za, ctx->st64.lam, ctx->st64.zp, s);
+        };
+    } else if (w == "stout_chain") {
+        f = [&]() {
+            if (m) launch_stout_chain<float>(g, ctx->U32, ctx->st32.lam, ctx->st32.zp, ctx->st32.za, s);
+            else launch_stout_chain<double>(g, ctx->U, ctx->st64.lam, ctx->st64.zp, ctx->st64.za, s);
+        };
+    } else if (w == "evolve") {
+        f = [&]() {
+            launch_evolve<double, double>(g, ctx->U, ctx->Ubak, ctx->P, 1e-3,
+                                          m ? ctx->Uaux32 : LinkPlanes<float>{nullptr, 0}, s);
+        };
+    } else if (w == "kick") {
+        f = [&]() {
+            if (m) launch_kick<float>(g, ctx->P, ctx->F32, 0.0, s);
+            else launch_kick<double>(g, ctx->P, ctx->F, 0.0, s);
+        };
+    } else if (w == "action") {
+        f = [&]() {
+            launch_action_sums<double>(g, ctx->U, true, ctx->partial, ctx->sums, SLOT_SCRATCH, SLOT_SCRATCH, s);
+        };
+    } else {
+        return fail(MAG_ERR_ARG, "mag_time_kernel: unknown kernel '" + w + "'");
+    }
+    f();
+    MAG_TRY(ctx->sync("mag_time_kernel warm-up"));
+    MAG_CUDA(cudaEventRecord(ctx->ev0, s));
+    for (int i = 0; i < reps; i++) f();
+    MAG_CUDA(cudaEventRecord(ctx->ev1, s));
+    MAG_TRY(ctx->sync("mag_time_kernel"));
+    float t = 0.f;
+    MAG_CUDA(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
+    *ms = t / reps;
+    return MAG_OK;
+}
+
+int mag_graph_kernel_count(mag_ctx* ctx, int* kernels) {
+    if (!ctx || !kernels) return MAG_ERR_ARG;
+    MAG_TRY(ctx->build_graph());
+    *kernels = ctx->graph_kernels;
+    return MAG_OK;
+}
+
+int mag_probe_fma_peak(int precision, double* tflops) {
+    if (!tflops || precision < 0 || precision > 1) return MAG_ERR_ARG;
+    int dev = 0, sms = 0;
+    MAG_CUDA(cudaGetDevice(&dev));
+    MAG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int nblocks = sms * 8, iters = precision == 0 ? 2048 : 8192;
+    void* out = nullptr;
+    MAG_CUDA(cudaMalloc(&out, (size_t)nblocks * 256 * 8));
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    for (int rep = 0; rep < 6; rep++) {
+        cudaEventRecord(a, 0);
+        if (precision == 0) launch_fma_probe<double>((double*)out, nblocks, iters, 0);
+        else launch_fma_probe<float>((float*)out, nblocks, iters, 0);
+        cudaEventRecord(b, 0);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0) best = std::min(best, ms);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    MAG_CUDA(cudaGetLastError());
+    *tflops = 2.0 * 8.0 * iters * (double)nblocks * 256 / (best * 1e-3) / 1e12;
+    return MAG_OK;
+}
+
+// closed paths summed over sites (or coarse sites) of one chain, double-double
+static int run_paths(mag_ctx* ctx, int chain, const std::vector<int>& dirs, int npath, int plen, int coarse_mag,
+                     double* sum) {
+    MAG_TRY(ctx->ensure_meas(1, 1, false));
+    if ((int)dirs.size() > ctx->max_path_ints) return fail(MAG_ERR_ARG, "path too long");
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_paths, dirs.data(), sizeof(int) * dirs.size(), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    launch_wilson_general(ctx->geom, ctx->U, ctx->d_paths, npath, plen, coarse_mag, ctx->wl_partial, ctx->wl_out,
+                          ctx->stream);
+    MAG_TRY(ctx->check("paths"));
+    std::vector<dd2> out(ctx->nchain);
+    MAG_CUDA(cudaMemcpyAsync(out.data(), ctx->wl_out, sizeof(dd2) * ctx->nchain, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    MAG_TRY(ctx->sync("paths"));
+    *sum = out[chain].hi + out[chain].lo;
+    return MAG_OK;
+}
+
+int mag_wilson_loop(mag_ctx* ctx, int chain, const int r[3], int T, double* out) {
+    if (!ctx || !r || !out || T < 1) return fail(MAG_ERR_ARG, "mag_wilson_loop: bad arguments");
+    MAG_TRY(ctx->chain_ok(chain));
+    for (int i = 0; i < 3; i++)
+        if (r[i] < 0) return fail(MAG_ERR_ARG, "mag_wilson_loop: negative r");
+    // permutations of the sorted r (field-wloop.h:66-71) and their paths (:32-50)
+    std::vector<int> rl(r, r + 3);
+    std::sort(rl.begin(), rl.end());
+    std::vector<std::vector<int>> paths;
+    do {
+        std::vector<int> d;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < rl[i]; j++) d.push_back(i);
+        for (int j = 0; j < T; j++) d.push_back(3);
+        for (int i = 2; i >= 0; i--)
+            for (int j = 0; j < rl[i]; j++) d.push_back(i + 4);
+        for (int j = 0; j < T; j++) d.push_back(7);
+        paths.push_back(d);
+    } while (std::next_permutation(rl.begin(), rl.end()));
+    const int plen = (int)paths[0].size();
+    std::vector<int> flat;
+    for (auto& p : paths) flat.insert(flat.end(), p.begin(), p.end());
+    double s = 0.0;
+    MAG_TRY(run_paths(ctx, chain, flat, (int)paths.size(), plen, 0, &s));
+    *out = s / ((double)paths.size() * ctx->hc[chain].V);
+    return MAG_OK;
+}
+
+int mag_wilson_loops(mag_ctx* ctx, int chain, int Rmax, int Tmax, double* out) {
+    if (!ctx || !out || Rmax < 1 || Tmax < 1 || Rmax > 64 || Tmax > 64)
+        return fail(MAG_ERR_ARG, "mag_wilson_loops: bad arguments");
+    MAG_TRY(ctx->chain_ok(chain));
+    MAG_TRY(ctx->ensure_meas(Rmax, Tmax, true));
+    const long vp = ctx->vpad;
+    LinkPlanes<double> lines{ctx->wl_lines, vp};
+    LinkPlanes<double> tl{ctx->wl_lines + (size_t)Rmax * 9 * vp, vp};
+    LinkPlanes<double> tl2{ctx->wl_lines + (size_t)(Rmax + 1) * 9 * vp, vp};
+    launch_wilson_planar(ctx->geom, ctx->U, Rmax, Tmax, lines, tl, tl2, ctx->wl_partial, ctx->wl_out, ctx->stream);
+    MAG_TRY(ctx->check("mag_wilson_loops"));
+    const size_t n = (size_t)3 * Tmax * ctx->nchain * Rmax;
+    std::vector<dd2> h(n);
+    MAG_CUDA(cudaMemcpyAsync(h.data(), ctx->wl_out, sizeof(dd2) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    MAG_TRY(ctx->sync("mag_wilson_loops"));
+    const double norm = 3.0 * ctx->hc[chain].V;  // perm.size() * V (field-wloop.h:98)
+    for (int R = 1; R <= Rmax; R++)
+        for (int T = 1; T <= Tmax; T++) {
+            hdd acc{0.0, 0.0};
+            for (int i = 0; i < 3; i++) {
+                const dd2 v = h[((size_t)(i * Tmax + T - 1) * ctx->nchain + chain) * Rmax + R - 1];
+                acc = h_add(acc, hdd{v.hi, v.lo});
+            }
+            out[(R - 1) * Tmax + (T - 1)] = (acc.hi + acc.lo) / norm;
+        }
+    return MAG_OK;
+}
+
+int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out) {
+    if (!ctx || !out) return MAG_ERR_ARG;
+    MAG_TRY(ctx->chain_ok(chain));
+    const int m = ctx->hc[chain].mag;
+    if (m < 1) return fail(MAG_ERR_STATE, "mag_constrained_plaquette: chain has no constraint (mag = 0)");
+    // mag x mag loops in the six planes mu > nu from every coarse site (field-matrix.h:418-436)
+    std::vector<int> flat;
+    int npath = 0;
+    for (int mu = 0; mu < 4; mu++)
+        for (int nu = 0; nu < mu; nu++) {
+            for (int i = 0; i < m; i++) flat.push_back(mu);
+            for (int i = 0; i < m; i++) flat.push_back(nu);
+            for (int i = 0; i < m; i++) flat.push_back(mu + 4);
+            for (int i = 0; i < m; i++) flat.push_back(nu + 4);
+            npath++;
+        }
+    double s = 0.0;
+    MAG_TRY(run_paths(ctx, chain, flat, npath, 4 * m, m, &s));
+    long coarse = 1;
+    for (int d = 0; d < 4; d++) coarse *= ctx->hc[chain].L[d] / m;
+    *out = s / (3.0 * (double)(coarse * npath));
+    return MAG_OK;
+}
+
+}  // extern "C"

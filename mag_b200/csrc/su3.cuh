@@ -1,0 +1,529 @@
+// su3.cuh -- SU(3) algebra for the constrained HMC kernels (float or double).
+//
+// A link is a 3x3 complex matrix (cps::Matrix in the reference, field-matrix.h).
+// Hermitian traceless matrices (momenta P, forces F, stout exponents Q, stout
+// Lambda) travel in a compact 8-real form
+//     h = (H00, H11, Re H01, Im H01, Re H02, Im H02, Re H12, Im H12),
+// with H22 = -H00 - H11 and the lower triangle conjugate-symmetric.
+#pragma once
+
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define MAG_HD __host__ __device__ __forceinline__
+#else
+#define MAG_HD inline
+#endif
+
+namespace magb {
+
+template <typename T>
+struct cplx {
+    T re, im;
+};
+
+template <typename T>
+MAG_HD cplx<T> mk(T r, T i) { cplx<T> c; c.re = r; c.im = i; return c; }
+template <typename T>
+MAG_HD cplx<T> operator+(cplx<T> a, cplx<T> b) { return mk(a.re + b.re, a.im + b.im); }
+template <typename T>
+MAG_HD cplx<T> operator-(cplx<T> a, cplx<T> b) { return mk(a.re - b.re, a.im - b.im); }
+template <typename T>
+MAG_HD cplx<T> operator*(cplx<T> a, cplx<T> b) { return mk(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+template <typename T>
+MAG_HD cplx<T> operator*(cplx<T> a, T s) { return mk(a.re * s, a.im * s); }
+template <typename T>
+MAG_HD cplx<T> conj(cplx<T> a) { return mk(a.re, -a.im); }
+
+template <typename T>
+struct mat3 {
+    cplx<T> e[3][3];
+};
+
+template <typename T>
+struct herm8 {
+    T h[8];
+};
+
+template <typename T>
+MAG_HD void set_zero(mat3<T>& m) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) m.e[i][j] = mk<T>(0, 0);
+}
+template <typename T>
+MAG_HD mat3<T> zero_mat() { mat3<T> m; set_zero(m); return m; }
+template <typename T>
+MAG_HD mat3<T> unit_mat() {
+    mat3<T> m;
+    set_zero(m);
+    m.e[0][0].re = m.e[1][1].re = m.e[2][2].re = T(1);
+    return m;
+}
+
+// c = a * b
+template <typename T>
+MAG_HD mat3<T> mul(const mat3<T>& a, const mat3<T>& b) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = a.e[i][0].re * b.e[0][j].re - a.e[i][0].im * b.e[0][j].im;
+            T im = a.e[i][0].re * b.e[0][j].im + a.e[i][0].im * b.e[0][j].re;
+#pragma unroll
+            for (int k = 1; k < 3; k++) {
+                re += a.e[i][k].re * b.e[k][j].re - a.e[i][k].im * b.e[k][j].im;
+                im += a.e[i][k].re * b.e[k][j].im + a.e[i][k].im * b.e[k][j].re;
+            }
+            c.e[i][j] = mk(re, im);
+        }
+    return c;
+}
+// c = a * b^dag
+template <typename T>
+MAG_HD mat3<T> mul_nd(const mat3<T>& a, const mat3<T>& b) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = a.e[i][0].re * b.e[j][0].re + a.e[i][0].im * b.e[j][0].im;
+            T im = -a.e[i][0].re * b.e[j][0].im + a.e[i][0].im * b.e[j][0].re;
+#pragma unroll
+            for (int k = 1; k < 3; k++) {
+                re += a.e[i][k].re * b.e[j][k].re + a.e[i][k].im * b.e[j][k].im;
+                im += -a.e[i][k].re * b.e[j][k].im + a.e[i][k].im * b.e[j][k].re;
+            }
+            c.e[i][j] = mk(re, im);
+        }
+    return c;
+}
+// c = a^dag * b
+template <typename T>
+MAG_HD mat3<T> mul_dn(const mat3<T>& a, const mat3<T>& b) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = a.e[0][i].re * b.e[0][j].re + a.e[0][i].im * b.e[0][j].im;
+            T im = a.e[0][i].re * b.e[0][j].im - a.e[0][i].im * b.e[0][j].re;
+#pragma unroll
+            for (int k = 1; k < 3; k++) {
+                re += a.e[k][i].re * b.e[k][j].re + a.e[k][i].im * b.e[k][j].im;
+                im += a.e[k][i].re * b.e[k][j].im - a.e[k][i].im * b.e[k][j].re;
+            }
+            c.e[i][j] = mk(re, im);
+        }
+    return c;
+}
+// acc += a * b
+template <typename T>
+MAG_HD void mul_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = acc.e[i][j].re, im = acc.e[i][j].im;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                re += a.e[i][k].re * b.e[k][j].re - a.e[i][k].im * b.e[k][j].im;
+                im += a.e[i][k].re * b.e[k][j].im + a.e[i][k].im * b.e[k][j].re;
+            }
+            acc.e[i][j] = mk(re, im);
+        }
+}
+// acc += a * b^dag
+template <typename T>
+MAG_HD void mul_nd_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = acc.e[i][j].re, im = acc.e[i][j].im;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                re += a.e[i][k].re * b.e[j][k].re + a.e[i][k].im * b.e[j][k].im;
+                im += -a.e[i][k].re * b.e[j][k].im + a.e[i][k].im * b.e[j][k].re;
+            }
+            acc.e[i][j] = mk(re, im);
+        }
+}
+// acc += a^dag * b
+template <typename T>
+MAG_HD void mul_dn_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            T re = acc.e[i][j].re, im = acc.e[i][j].im;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                re += a.e[k][i].re * b.e[k][j].re + a.e[k][i].im * b.e[k][j].im;
+                im += a.e[k][i].re * b.e[k][j].im - a.e[k][i].im * b.e[k][j].re;
+            }
+            acc.e[i][j] = mk(re, im);
+        }
+}
+
+template <typename T>
+MAG_HD mat3<T> adj(const mat3<T>& a) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) c.e[i][j] = conj(a.e[j][i]);
+    return c;
+}
+template <typename T>
+MAG_HD void add_to(mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) a.e[i][j] = a.e[i][j] + b.e[i][j];
+}
+template <typename T>
+MAG_HD void sub_from(mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) a.e[i][j] = a.e[i][j] - b.e[i][j];
+}
+// a += s * b
+template <typename T>
+MAG_HD void axpy(mat3<T>& a, T s, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            a.e[i][j].re += s * b.e[i][j].re;
+            a.e[i][j].im += s * b.e[i][j].im;
+        }
+}
+// a += z * b (complex scalar)
+template <typename T>
+MAG_HD void caxpy(mat3<T>& a, cplx<T> z, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) a.e[i][j] = a.e[i][j] + z * b.e[i][j];
+}
+template <typename T>
+MAG_HD mat3<T> scaled(const mat3<T>& a, T s) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) c.e[i][j] = a.e[i][j] * s;
+    return c;
+}
+// i * s * a
+template <typename T>
+MAG_HD mat3<T> times_i(const mat3<T>& a, T s) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) c.e[i][j] = mk(-s * a.e[i][j].im, s * a.e[i][j].re);
+    return c;
+}
+template <typename T>
+MAG_HD T retr(const mat3<T>& a) { return a.e[0][0].re + a.e[1][1].re + a.e[2][2].re; }
+// Re Tr(a * b) without forming the product
+template <typename T>
+MAG_HD T retr_mul(const mat3<T>& a, const mat3<T>& b) {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) s += a.e[i][k].re * b.e[k][i].re - a.e[i][k].im * b.e[k][i].im;
+    return s;
+}
+// Tr(a * b)
+template <typename T>
+MAG_HD cplx<T> tr_mul(const mat3<T>& a, const mat3<T>& b) {
+    cplx<T> s = mk<T>(0, 0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) s = s + a.e[i][k] * b.e[k][i];
+    return s;
+}
+template <typename T, typename S>
+MAG_HD mat3<T> convert(const mat3<S>& a) {
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) c.e[i][j] = mk<T>((T)a.e[i][j].re, (T)a.e[i][j].im);
+    return c;
+}
+
+// ---------------------------------------------------------- compact Hermitian
+template <typename T>
+MAG_HD mat3<T> expand(const herm8<T>& q) {
+    mat3<T> m;
+    m.e[0][0] = mk<T>(q.h[0], 0);
+    m.e[1][1] = mk<T>(q.h[1], 0);
+    m.e[2][2] = mk<T>(-q.h[0] - q.h[1], 0);
+    m.e[0][1] = mk<T>(q.h[2], q.h[3]);
+    m.e[1][0] = mk<T>(q.h[2], -q.h[3]);
+    m.e[0][2] = mk<T>(q.h[4], q.h[5]);
+    m.e[2][0] = mk<T>(q.h[4], -q.h[5]);
+    m.e[1][2] = mk<T>(q.h[6], q.h[7]);
+    m.e[2][1] = mk<T>(q.h[6], -q.h[7]);
+    return m;
+}
+// compact of a matrix that is Hermitian traceless by construction (upper triangle read)
+template <typename T>
+MAG_HD herm8<T> compact(const mat3<T>& m) {
+    herm8<T> q;
+    q.h[0] = m.e[0][0].re; q.h[1] = m.e[1][1].re;
+    q.h[2] = m.e[0][1].re; q.h[3] = m.e[0][1].im;
+    q.h[4] = m.e[0][2].re; q.h[5] = m.e[0][2].im;
+    q.h[6] = m.e[1][2].re; q.h[7] = m.e[1][2].im;
+    return q;
+}
+template <typename T>
+MAG_HD herm8<T> herm_zero() { herm8<T> q; for (int k = 0; k < 8; k++) q.h[k] = T(0); return q; }
+template <typename T>
+MAG_HD herm8<T> scaled(const herm8<T>& a, T s) { herm8<T> q; for (int k = 0; k < 8; k++) q.h[k] = a.h[k] * s; return q; }
+
+// F = i s TA(M),  TA(M) = 1/2 (M - M^dag) - 1/6 Tr(M - M^dag)  (cps TrLessAntiHermMatrix)
+template <typename T>
+MAG_HD herm8<T> i_times_ta(const mat3<T>& m, T s) {
+    const T t = (m.e[0][0].im + m.e[1][1].im + m.e[2][2].im) / T(3);
+    herm8<T> q;
+    q.h[0] = -s * (m.e[0][0].im - t);
+    q.h[1] = -s * (m.e[1][1].im - t);
+    // off-diagonal TA_ij = (1/2 (Re M_ij - Re M_ji), 1/2 (Im M_ij + Im M_ji)); times i s
+    q.h[2] = -s * (T(0.5) * (m.e[0][1].im + m.e[1][0].im));
+    q.h[3] = s * (T(0.5) * (m.e[0][1].re - m.e[1][0].re));
+    q.h[4] = -s * (T(0.5) * (m.e[0][2].im + m.e[2][0].im));
+    q.h[5] = s * (T(0.5) * (m.e[0][2].re - m.e[2][0].re));
+    q.h[6] = -s * (T(0.5) * (m.e[1][2].im + m.e[2][1].im));
+    q.h[7] = s * (T(0.5) * (m.e[1][2].re - m.e[2][1].re));
+    return q;
+}
+// Lambda = 1/2 (G + G^dag) - 1/6 Tr(G + G^dag)  (field-multi.h:41-45)
+template <typename T>
+MAG_HD herm8<T> herm_traceless(const mat3<T>& g) {
+    const T t = (g.e[0][0].re + g.e[1][1].re + g.e[2][2].re) / T(3);
+    herm8<T> q;
+    q.h[0] = g.e[0][0].re - t;
+    q.h[1] = g.e[1][1].re - t;
+    q.h[2] = T(0.5) * (g.e[0][1].re + g.e[1][0].re);
+    q.h[3] = T(0.5) * (g.e[0][1].im - g.e[1][0].im);
+    q.h[4] = T(0.5) * (g.e[0][2].re + g.e[2][0].re);
+    q.h[5] = T(0.5) * (g.e[0][2].im - g.e[2][0].im);
+    q.h[6] = T(0.5) * (g.e[1][2].re + g.e[2][1].re);
+    q.h[7] = T(0.5) * (g.e[1][2].im - g.e[2][1].im);
+    return q;
+}
+// Re Tr(H^2) of a compact Hermitian traceless matrix
+template <typename T>
+MAG_HD T retr_sq(const herm8<T>& q) {
+    const T h22 = -q.h[0] - q.h[1];
+    return q.h[0] * q.h[0] + q.h[1] * q.h[1] + h22 * h22 +
+           T(2) * (q.h[2] * q.h[2] + q.h[3] * q.h[3] + q.h[4] * q.h[4] + q.h[5] * q.h[5] + q.h[6] * q.h[6] +
+                   q.h[7] * q.h[7]);
+}
+
+// CPS Matrix::Unitarize: normalise row 0, orthogonalise row 1 to it and
+// normalise, row 2 = conj(row0 x row1).
+template <typename T>
+MAG_HD void unitarize(mat3<T>& m) {
+    T n0 = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) n0 += m.e[0][k].re * m.e[0][k].re + m.e[0][k].im * m.e[0][k].im;
+    n0 = T(1) / sqrt(n0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) m.e[0][k] = m.e[0][k] * n0;
+    cplx<T> c = mk<T>(0, 0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) c = c + conj(m.e[0][k]) * m.e[1][k];
+#pragma unroll
+    for (int k = 0; k < 3; k++) m.e[1][k] = m.e[1][k] - c * m.e[0][k];
+    T n1 = T(0);
+#pragma unroll
+    for (int k = 0; k < 3; k++) n1 += m.e[1][k].re * m.e[1][k].re + m.e[1][k].im * m.e[1][k].im;
+    n1 = T(1) / sqrt(n1);
+#pragma unroll
+    for (int k = 0; k < 3; k++) m.e[1][k] = m.e[1][k] * n1;
+    m.e[2][0] = conj(m.e[0][1] * m.e[1][2] - m.e[0][2] * m.e[1][1]);
+    m.e[2][1] = conj(m.e[0][2] * m.e[1][0] - m.e[0][0] * m.e[1][2]);
+    m.e[2][2] = conj(m.e[0][0] * m.e[1][1] - m.e[0][1] * m.e[1][0]);
+}
+
+// -------------------------------------------------- Cayley-Hamilton exp(iQ)
+// Scalar part of hep-lat/0311018 as written in field-hmc.h:88-115 (expiQ) and
+// field-multi.h:92-168 (DexpiQ / compute_Lambda).  Always evaluated in double:
+// the FP32 kernels call it too, because the f_j and b_ij formulas cancel
+// catastrophically in single precision.
+struct ch_coef {
+    int trivial;  // c1 == 0: expiQ = 1, derivative terms = 0
+    double f0r, f0i, f1r, f1i, f2r, f2i;
+    double b10r, b10i, b11r, b11i, b12r, b12i;
+    double b20r, b20i, b21r, b21i, b22r, b22i;
+};
+
+// c0 = Re Tr(Q^3)/3, c1 = Re Tr(Q^2)/2 as supplied by the caller.
+template <bool WITH_B>
+MAG_HD ch_coef ch_coefficients(double c0, double c1) {
+    ch_coef r;
+    r.trivial = 0;
+    bool reflect = false;
+    if (c0 < 0.0) { c0 = -c0; reflect = true; }
+    if (c1 == 0.0) {
+        r.trivial = 1;
+        r.f0r = 1.0; r.f0i = r.f1r = r.f1i = r.f2r = r.f2i = 0.0;
+        r.b10r = r.b10i = r.b11r = r.b11i = r.b12r = r.b12i = 0.0;
+        r.b20r = r.b20i = r.b21r = r.b21i = r.b22r = r.b22i = 0.0;
+        return r;
+    }
+    const double c0m = 2.0 * pow(c1 / 3.0, 1.5);
+    double ratio = c0 / c0m;
+    if (ratio > 1.0) ratio = 1.0;  // rounding guard (reference would return NaN)
+    const double theta = acos(ratio);
+    const double u = sqrt(c1 / 3.0) * cos(theta / 3.0);
+    const double w = sqrt(c1) * sin(theta / 3.0);
+    const double ww = w * w, uu = u * u;
+    double xi0, xi1 = 0.0;
+    if (ww < 0.05 * 0.05) {
+        xi0 = 1. - ww / 6. * (1. - ww / 20. * (1. - ww / 42.));
+        if (WITH_B) xi1 = -1. / 2. * (1. - ww / 12. * (1. - ww / 30.)) + 1. / 6. * (1. - ww / 20. * (1. - ww / 42.));
+    } else {
+        const double sw = sin(w);
+        xi0 = sw / w;
+        if (WITH_B) xi1 = cos(w) / ww - sw / (ww * w);
+    }
+    const double cw = cos(w);
+    const double c2u = cos(2. * u), s2u = sin(2. * u);
+    const double cu = cos(u), su = sin(u);
+    // e2u = exp(2iu), emu = exp(-iu)
+    // h0 = (u^2-w^2) e2u + emu (8u^2 cos w + i 2u(3u^2+w^2) xi0)
+    const double a0r = 8. * uu * cw, a0i = 2. * u * (3. * uu + ww) * xi0;
+    const double h0r = (uu - ww) * c2u + (cu * a0r + su * a0i);
+    const double h0i = (uu - ww) * s2u + (cu * a0i - su * a0r);
+    // h1 = 2u e2u - emu (2u cos w - i (3u^2-w^2) xi0)
+    const double a1r = 2. * u * cw, a1i = -(3. * uu - ww) * xi0;
+    const double h1r = 2. * u * c2u - (cu * a1r + su * a1i);
+    const double h1i = 2. * u * s2u - (cu * a1i - su * a1r);
+    // h2 = e2u - emu (cos w + i 3u xi0)
+    const double a2r = cw, a2i = 3. * u * xi0;
+    const double h2r = c2u - (cu * a2r + su * a2i);
+    const double h2i = s2u - (cu * a2i - su * a2r);
+    const double den = 9. * uu - ww;
+    double f0r = h0r / den, f0i = h0i / den, f1r = h1r / den, f1i = h1i / den, f2r = h2r / den, f2i = h2i / den;
+    if (WITH_B) {
+        // complex helpers in (re, im) pairs
+        // r01 = 2(u + i(u^2-w^2)) e2u + 2 emu (4u(2 - iu) cos w + i xi0 (9u^2 + w^2 - iu(3u^2+w^2)))
+        double tr_, ti_;
+        // term A = 2(u + i(uu-ww)) * e2u
+        const double Ar = 2. * (u * c2u - (uu - ww) * s2u), Ai = 2. * (u * s2u + (uu - ww) * c2u);
+        // inner B = 4u(2 - iu) cw + i xi0 (9uu + ww - iu(3uu+ww))
+        //         = (8u cw + xi0 u (3uu+ww)) + i(-4uu cw + xi0 (9uu + ww))
+        const double Br = 8. * u * cw + xi0 * u * (3. * uu + ww), Bi = -4. * uu * cw + xi0 * (9. * uu + ww);
+        tr_ = 2. * (cu * Br + su * Bi); ti_ = 2. * (cu * Bi - su * Br);
+        const double r01r = Ar + tr_, r01i = Ai + ti_;
+        // r11 = 2(1 + 2iu) e2u + emu(-2(1 - iu) cw + i xi0 (6u + i(ww - 3uu)))
+        const double Cr = 2. * (c2u - 2. * u * s2u), Ci = 2. * (s2u + 2. * u * c2u);
+        // inner D = -2cw + 2iu cw + i 6u xi0 - xi0 (ww - 3uu)
+        const double Dr = -2. * cw - xi0 * (ww - 3. * uu), Di = 2. * u * cw + 6. * u * xi0;
+        const double r11r = Cr + (cu * Dr + su * Di), r11i = Ci + (cu * Di - su * Dr);
+        // r21 = 2i e2u + i emu (cw - 3 xi0 (1 - iu))
+        //   inner E = (cw - 3xi0) + i 3u xi0 ; i*emu*E
+        const double Er = cw - 3. * xi0, Ei = 3. * u * xi0;
+        const double eEr = cu * Er + su * Ei, eEi = cu * Ei - su * Er;
+        const double r21r = -2. * s2u - eEi, r21i = 2. * c2u + eEr;
+        // r02 = -2 e2u + 2iu emu (cw + (1 + 4iu) xi0 + 3uu xi1)
+        const double Fr = cw + xi0 + 3. * uu * xi1, Fi = 4. * u * xi0;
+        const double eFr = cu * Fr + su * Fi, eFi = cu * Fi - su * Fr;
+        const double r02r = -2. * c2u - 2. * u * eFi, r02i = -2. * s2u + 2. * u * eFr;
+        // r12 = -i emu (cw + (1 + 2iu) xi0 - 3uu xi1)
+        const double Gr = cw + xi0 - 3. * uu * xi1, Gi = 2. * u * xi0;
+        const double eGr = cu * Gr + su * Gi, eGi = cu * Gi - su * Gr;
+        const double r12r = eGi, r12i = -eGr;
+        // r22 = emu (xi0 - 3iu xi1)
+        const double Hr = xi0, Hi = -3. * u * xi1;
+        const double r22r = cu * Hr + su * Hi, r22i = cu * Hi - su * Hr;
+        const double bden = 2. * den * den;
+        const double k1 = 3. * uu - ww, k2 = 2. * (15. * uu + ww);
+        r.b10r = (2. * u * r01r + k1 * r02r - k2 * f0r) / bden;
+        r.b10i = (2. * u * r01i + k1 * r02i - k2 * f0i) / bden;
+        r.b11r = (2. * u * r11r + k1 * r12r - k2 * f1r) / bden;
+        r.b11i = (2. * u * r11i + k1 * r12i - k2 * f1i) / bden;
+        r.b12r = (2. * u * r21r + k1 * r22r - k2 * f2r) / bden;
+        r.b12i = (2. * u * r21i + k1 * r22i - k2 * f2i) / bden;
+        r.b20r = (r01r - 3. * u * r02r - 24. * u * f0r) / bden;
+        r.b20i = (r01i - 3. * u * r02i - 24. * u * f0i) / bden;
+        r.b21r = (r11r - 3. * u * r12r - 24. * u * f1r) / bden;
+        r.b21i = (r11i - 3. * u * r12i - 24. * u * f1i) / bden;
+        r.b22r = (r21r - 3. * u * r22r - 24. * u * f2r) / bden;
+        r.b22i = (r21i - 3. * u * r22i - 24. * u * f2i) / bden;
+        if (reflect) {
+            r.b10i = -r.b10i;                 // conj
+            r.b11r = -r.b11r;                 // -conj
+            r.b12i = -r.b12i;                 // conj
+            r.b20r = -r.b20r;                 // -conj
+            r.b21i = -r.b21i;                 // conj
+            r.b22r = -r.b22r;                 // -conj
+        }
+    } else {
+        r.b10r = r.b10i = r.b11r = r.b11i = r.b12r = r.b12i = 0.0;
+        r.b20r = r.b20i = r.b21r = r.b21i = r.b22r = r.b22i = 0.0;
+    }
+    if (reflect) {
+        f0i = -f0i;    // conj
+        f1r = -f1r;    // -conj
+        f2i = -f2i;    // conj
+    }
+    r.f0r = f0r; r.f0i = f0i; r.f1r = f1r; r.f1i = f1i; r.f2r = f2r; r.f2i = f2i;
+    return r;
+}
+
+// Q^2 of a compact Hermitian traceless matrix (Hermitian result)
+template <typename T>
+MAG_HD mat3<T> herm_square(const herm8<T>& q) {
+    const mat3<T> Q = expand(q);
+    return mul(Q, Q);
+}
+
+// c0 = Re Tr(Q^3)/3 and c1 = Re Tr(Q^2)/2 in double (as field-hmc.h:88-94)
+template <typename T>
+MAG_HD void ch_invariants(const mat3<T>& Q, const mat3<T>& QQ, double& c0, double& c1) {
+    double t3 = 0.0, t2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        t2 += (double)QQ.e[i][i].re;
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+            t3 += (double)QQ.e[i][k].re * (double)Q.e[k][i].re - (double)QQ.e[i][k].im * (double)Q.e[k][i].im;
+    }
+    c0 = t3 / 3.0;
+    c1 = t2 / 2.0;
+}
+
+// exp(iQ) = f0 + f1 Q + f2 Q^2 (field-hmc.h:82-123)
+template <typename T>
+MAG_HD mat3<T> expiQ(const herm8<T>& q) {
+    const mat3<T> Q = expand(q);
+    const mat3<T> QQ = mul(Q, Q);
+    double c0, c1;
+    ch_invariants(Q, QQ, c0, c1);
+    const ch_coef c = ch_coefficients<false>(c0, c1);
+    if (c.trivial) return unit_mat<T>();
+    mat3<T> r;
+    const cplx<T> f1 = mk<T>((T)c.f1r, (T)c.f1i), f2 = mk<T>((T)c.f2r, (T)c.f2i);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) r.e[i][j] = f1 * Q.e[i][j] + f2 * QQ.e[i][j];
+#pragma unroll
+    for (int i = 0; i < 3; i++) r.e[i][i] = r.e[i][i] + mk<T>((T)c.f0r, (T)c.f0i);
+    return r;
+}
+
+}  // namespace magb

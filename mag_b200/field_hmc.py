@@ -1,0 +1,272 @@
+"""Host-side mirror of mag's field-*.h operator surface over libmag_b200.so.
+
+The reference is header-only C++ (field-hmc.h, field-matrix.h, field-multi.h,
+field-wloop.h, field-demon.h) with free functions over ``Field<cps::Matrix>``.
+Here one ``Chmc`` object owns the device fields of one lattice (or of an
+ensemble of chains) and exposes the same operations under the same names;
+fields cross the boundary as numpy arrays of shape (V, 4, 3, 3) complex128,
+the reference's AoS layout with x0 fastest.
+
+Errors raise ``MagError`` (the reference asserts and aborts).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import MagParams, TrajResult, check
+
+_ACTIONS = {"wilson": _lib.ACTION_WILSON, "iwasaki": _lib.ACTION_IWASAKI}
+_PREC = {"fp64": _lib.PREC_FP64, "mixed": _lib.PREC_MIXED}
+_INTEG = {"fg": _lib.INT_FORCE_GRADIENT, "force_gradient": _lib.INT_FORCE_GRADIENT,
+          "leapfrog": _lib.INT_LEAPFROG}
+_ACCEPT = {"metropolis": _lib.ACCEPT_METROPOLIS, "demon": _lib.ACCEPT_DEMON}
+
+
+def volume(dims: Sequence[int]) -> int:
+    v = 1
+    for d in dims:
+        v *= int(d)
+    return v
+
+
+def make_params(dims, mag=2, action="iwasaki", beta=2.25, c1=-0.331, rho=0.1, n_stout=0, tau=1.0, n_steps=8,
+                precision="fp64", integrator="fg", accept="metropolis", e_max=100.0, n_forced_accept=0,
+                seed=1) -> MagParams:
+    """Arg_chmc (field-hmc.h:294-307) + qlat::Gauge + run options."""
+    p = MagParams()
+    p.dims[:] = [int(d) for d in dims]
+    p.mag = int(mag)
+    p.action = _ACTIONS[action] if isinstance(action, str) else int(action)
+    p.beta, p.c1, p.rho = float(beta), float(c1), float(rho)
+    p.n_stout = int(n_stout)
+    p.tau, p.n_steps = float(tau), int(n_steps)
+    p.precision = _PREC[precision] if isinstance(precision, str) else int(precision)
+    p.integrator = _INTEG[integrator] if isinstance(integrator, str) else int(integrator)
+    p.accept = _ACCEPT[accept] if isinstance(accept, str) else int(accept)
+    p.e_max = float(e_max)
+    p.n_forced_accept = int(n_forced_accept)
+    p.seed = int(seed)
+    return p
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.complex128 or a.dtype == np.float64
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Chmc:
+    """Device-resident constrained HMC state (run_chmc's fields, field-hmc.h:770-784)."""
+
+    def __init__(self, dims=None, *, chains: Iterable[dict] | None = None, **kw):
+        self._lib = _lib.load()
+        if chains is None:
+            plist = [make_params(dims, **kw)]
+        else:
+            plist = [make_params(**{**kw, **c}) for c in chains]
+        self.params = plist
+        self.dims = [tuple(p.dims) for p in plist]
+        arr = (MagParams * len(plist))(*plist)
+        h = ctypes.c_void_p()
+        check(self._lib.mag_ensemble_create(arr, len(plist), ctypes.byref(h)), "mag_ensemble_create")
+        self._h = h
+        self.n_chains = len(plist)
+
+    # ------------------------------------------------------------ lifecycle
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.mag_ctx_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def volume(self, chain: int = 0) -> int:
+        return volume(self.dims[chain])
+
+    def _field(self, chain: int) -> np.ndarray:
+        return np.zeros((self.volume(chain), 4, 3, 3), np.complex128)
+
+    def device_bytes(self) -> int:
+        b = ctypes.c_size_t()
+        check(self._lib.mag_ctx_device_bytes(self._h, ctypes.byref(b)), "mag_ctx_device_bytes")
+        return b.value
+
+    # ------------------------------------------------------------ field I/O
+    def set_gauge(self, U: np.ndarray, chain: int = 0) -> None:
+        U = np.ascontiguousarray(U, np.complex128)
+        assert U.shape == (self.volume(chain), 4, 3, 3)
+        check(self._lib.mag_gauge_set(self._h, chain, _dp(U)), "mag_gauge_set")
+
+    def get_gauge(self, chain: int = 0) -> np.ndarray:
+        U = self._field(chain)
+        check(self._lib.mag_gauge_get(self._h, chain, _dp(U)), "mag_gauge_get")
+        return U
+
+    def hot_start(self, seed: int) -> None:
+        check(self._lib.mag_gauge_hot_start(self._h, int(seed)), "mag_gauge_hot_start")
+
+    def cold_start(self) -> None:
+        check(self._lib.mag_gauge_cold_start(self._h), "mag_gauge_cold_start")
+
+    def init_momentum(self, P: np.ndarray | None = None, chain: int = 0, traj: int = 0) -> None:
+        """init_momentum (field-hmc.h:675): host momenta, or Philox momenta of trajectory ``traj``."""
+        if P is None:
+            check(self._lib.mag_momentum_refresh(self._h, int(traj)), "mag_momentum_refresh")
+            return
+        P = np.ascontiguousarray(P, np.complex128)
+        check(self._lib.mag_momentum_set(self._h, chain, _dp(P)), "mag_momentum_set")
+
+    def get_momentum(self, chain: int = 0) -> np.ndarray:
+        P = self._field(chain)
+        check(self._lib.mag_momentum_get(self._h, chain, _dp(P)), "mag_momentum_get")
+        return P
+
+    def set_uniforms(self, u: Sequence[float] | None) -> None:
+        if u is None:
+            check(self._lib.mag_uniforms_set(self._h, None), "mag_uniforms_set")
+            return
+        a = np.ascontiguousarray(np.asarray(u, np.float64).reshape(self.n_chains))
+        check(self._lib.mag_uniforms_set(self._h, _dp(a)), "mag_uniforms_set")
+
+    # ------------------------------------------------------------ operators
+    def get_force(self, chain: int = 0) -> np.ndarray:
+        """get_force (field-hmc.h:339-425), through the stout chain when n_stout > 0."""
+        F = self._field(chain)
+        check(self._lib.mag_gauge_force(self._h, chain, _dp(F)), "mag_gauge_force")
+        return F
+
+    def get_extended_staple_dagger(self, chain: int = 0) -> np.ndarray:
+        """get_extended_staple_dagger (field-hmc.h:262-269) of every link of the smeared field."""
+        V = self._field(chain)
+        check(self._lib.mag_staple(self._h, chain, _dp(V)), "mag_staple")
+        return V
+
+    def gauge_action(self, chain: int = 0):
+        """(total_plaq, total_rectangular, S) of the smeared links (field-matrix.h:299-385, field-hmc.h:632-639)."""
+        p, r, s = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(self._lib.mag_action(self._h, chain, ctypes.byref(p), ctypes.byref(r), ctypes.byref(s)), "mag_action")
+        return p.value, r.value, s.value
+
+    def total_plaq(self, chain: int = 0) -> float:
+        return self.gauge_action(chain)[0]
+
+    def total_rectangular(self, chain: int = 0) -> float:
+        return self.gauge_action(chain)[1]
+
+    def avg_plaquette(self, chain: int = 0) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_plaquette(self._h, chain, ctypes.byref(v)), "mag_plaquette")
+        return v.value
+
+    def kinetic_energy(self, chain: int = 0) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_kinetic(self._h, chain, ctypes.byref(v)), "mag_kinetic")
+        return v.value
+
+    def get_hamiltonian(self, chain: int = 0):
+        """get_hamiltonian (field-hmc.h:589-644): returns (H, [kinetic, potential])."""
+        out = np.zeros(3)
+        check(self._lib.mag_hamiltonian(self._h, chain, _dp(out)), "mag_hamiltonian")
+        return float(out[0]), [float(out[1]), float(out[2])]
+
+    def evolve_gauge_field(self, dt: float) -> None:
+        check(self._lib.mag_evolve_gauge(self._h, float(dt)), "mag_evolve_gauge")
+
+    def evolve_momentum(self, dt: float) -> None:
+        check(self._lib.mag_evolve_momentum(self._h, float(dt)), "mag_evolve_momentum")
+
+    def force_gradient_integrator(self) -> None:
+        """force_gradient_integrator (field-hmc.h:525-567) or leap_frog_integrator per the params."""
+        check(self._lib.mag_integrate(self._h), "mag_integrate")
+
+    def reunitarize(self) -> list:
+        out = np.zeros(self.n_chains)
+        check(self._lib.mag_reunitarize(self._h, _dp(out)), "mag_reunitarize")
+        return [float(v) for v in out]
+
+    def stout_level(self, level: int, chain: int = 0) -> np.ndarray:
+        U = self._field(chain)
+        check(self._lib.mag_stout_level(self._h, chain, int(level), _dp(U)), "mag_stout_level")
+        return U
+
+    # ------------------------------------------------------------ HMC
+    def trajectory(self, refresh_momenta: bool = True) -> list:
+        """One run_chmc trajectory (field-hmc.h:806-843) of every chain."""
+        res = (TrajResult * self.n_chains)()
+        check(self._lib.mag_trajectory(self._h, 1 if refresh_momenta else 0, res), "mag_trajectory")
+        return [r.as_dict() for r in res]
+
+    def run_chmc(self, n_traj: int) -> list:
+        """n trajectories replayed as CUDA graphs; returns [traj][chain] records."""
+        res = (TrajResult * (n_traj * self.n_chains))()
+        check(self._lib.mag_run(self._h, int(n_traj), res), "mag_run")
+        return [[res[t * self.n_chains + c].as_dict() for c in range(self.n_chains)] for t in range(n_traj)]
+
+    def traj_counter(self) -> int:
+        v = ctypes.c_int64()
+        check(self._lib.mag_traj_counter(self._h, ctypes.byref(v)), "mag_traj_counter")
+        return v.value
+
+    def set_traj_counter(self, t: int) -> None:
+        check(self._lib.mag_set_traj_counter(self._h, int(t)), "mag_set_traj_counter")
+
+    # ------------------------------------------------------------ measurement
+    def avg_wilson_loop(self, r: Sequence[int], T: int, chain: int = 0) -> float:
+        """avg_wilson_loop (field-wloop.h:58-99)."""
+        rr = (ctypes.c_int * 3)(*[int(v) for v in r])
+        v = ctypes.c_double()
+        check(self._lib.mag_wilson_loop(self._h, chain, rr, int(T), ctypes.byref(v)), "mag_wilson_loop")
+        return v.value
+
+    def wilson_loops(self, Rmax: int, Tmax: int, chain: int = 0) -> np.ndarray:
+        """Planar loops W[R-1, T-1] = avg_wilson_loop((R,0,0), T) for R <= Rmax, T <= Tmax."""
+        out = np.zeros((Rmax, Tmax))
+        check(self._lib.mag_wilson_loops(self._h, chain, int(Rmax), int(Tmax), _dp(out)), "mag_wilson_loops")
+        return out
+
+    def check_constrained_plaquette(self, chain: int = 0) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_constrained_plaquette(self._h, chain, ctypes.byref(v)), "mag_constrained_plaquette")
+        return v.value
+
+    # ------------------------------------------------------------ timing
+    def last_run_ms(self) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_last_run_ms(self._h, ctypes.byref(v)), "mag_last_run_ms")
+        return v.value
+
+    def time_force(self, reps: int) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_time_force(self._h, int(reps), ctypes.byref(v)), "mag_time_force")
+        return v.value
+
+    def time_kernel(self, which: str, reps: int) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_time_kernel(self._h, which.encode(), int(reps), ctypes.byref(v)), "mag_time_kernel")
+        return v.value
+
+    def graph_kernel_count(self) -> int:
+        v = ctypes.c_int()
+        check(self._lib.mag_graph_kernel_count(self._h, ctypes.byref(v)), "mag_graph_kernel_count")
+        return v.value
+
+
+def probe_fma_peak(precision: str = "fp64") -> float:
+    """Measured CUDA-core FMA throughput of the current device (TFLOP/s, 2 flops per FMA)."""
+    v = ctypes.c_double()
+    check(_lib.load().mag_probe_fma_peak(0 if precision == "fp64" else 1, ctypes.byref(v)), "mag_probe_fma_peak")
+    return v.value

@@ -1,0 +1,269 @@
+"""GPU parity: libmag_b200.so (sm_100a kernels, through the C ABI) against the
+FP64 CPU oracle on the same seeded inputs.
+
+Tolerances (plain FP64 GPU path): plaquette/action 1e-12 relative, per-link
+force 1e-11 (relative to the largest force component), Delta H 1e-9
+absolute, identical accept/reject and demon sequences.  Mixed precision
+(FP32 staples/force/smearing on FP32 copies of FP64 master links): force 5e-5
+relative, Delta H within 2e-2 of the FP64 path on the same trajectory.
+"""
+import numpy as np
+import pytest
+
+import mag_b200 as M
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+DIMS = (4, 4, 4, 6)
+
+
+def maxrel(a, b):
+    return np.abs(a - b).max() / max(1.0, np.abs(b).max())
+
+
+def test_gauge_roundtrip_and_device_rng():
+    with M.Chmc(DIMS, seed=21) as c:
+        U = O.gen_hot(DIMS, 5)
+        c.set_gauge(U)
+        assert np.array_equal(c.get_gauge(), U)
+        c.hot_start(5)
+        assert np.abs(c.get_gauge() - U).max() < 1e-13
+        c.init_momentum(None, traj=3)
+        assert np.abs(c.get_momentum() - O.gen_momenta(DIMS, 21, 3)).max() < 1e-13
+        P = O.gen_momenta(DIMS, 8, 0)
+        c.init_momentum(P)
+        assert np.abs(c.get_momentum() - P).max() < 1e-15
+
+
+@pytest.mark.parametrize("action,mag,n_stout", [
+    ("iwasaki", 0, 0), ("wilson", 0, 0), ("iwasaki", 2, 0), ("wilson", 2, 0),
+    ("iwasaki", 0, 1), ("iwasaki", 0, 3), ("iwasaki", 2, 3), ("wilson", 2, 1)])
+def test_force_parity_fp64(action, mag, n_stout):
+    U = O.gen_hot(DIMS, 7)
+    po = O.make_params(DIMS, mag=mag, action=1 if action == "iwasaki" else 0, n_stout=n_stout, rho=0.1)
+    with M.Chmc(DIMS, mag=mag, action=action, n_stout=n_stout, rho=0.1) as c:
+        c.set_gauge(U)
+        F = c.get_force()
+    Fo = O.force(po, U)
+    assert maxrel(F, Fo) < 1e-11
+
+
+@pytest.mark.parametrize("action", ["iwasaki", "wilson"])
+def test_staple_and_action_parity(action):
+    U = O.gen_hot(DIMS, 9)
+    a = 1 if action == "iwasaki" else 0
+    po = O.make_params(DIMS, action=a)
+    with M.Chmc(DIMS, action=action, mag=0) as c:
+        c.set_gauge(U)
+        V = c.get_extended_staple_dagger()
+        p, r, s = c.gauge_action()
+        avg = c.avg_plaquette()
+    assert maxrel(V, O.staple_dagger(po, U)) < 1e-12
+    po_, ro_, so_ = O.action(po, U)
+    assert abs(p - po_) <= 1e-12 * abs(po_) + 1e-12
+    assert abs(r - ro_) <= 1e-12 * abs(ro_) + 1e-12
+    assert abs(s - so_) <= 1e-12 * abs(so_)
+    assert abs(avg - O.avg_plaquette(DIMS, U)) < 1e-14
+
+
+def test_smeared_action_and_levels_parity():
+    U = O.gen_hot(DIMS, 10)
+    po = O.make_params(DIMS, n_stout=3, rho=0.1)
+    lv = O.stout_forward(po, U)
+    with M.Chmc(DIMS, n_stout=3, rho=0.1) as c:
+        c.set_gauge(U)
+        for k in range(4):
+            assert np.abs(c.stout_level(k) - lv[k]).max() < 1e-13
+        p, r, s = c.gauge_action()
+    po_, ro_, so_ = O.action(po, U)
+    assert abs(s - so_) <= 1e-12 * abs(so_)
+    assert abs(p - po_) <= 1e-12 * abs(po_)
+
+
+@pytest.mark.parametrize("mag", [0, 2])
+def test_hamiltonian_and_updates_parity(mag):
+    U = O.gen_hot(DIMS, 11)
+    P = O.gen_momenta(DIMS, 3, 0)
+    po = O.make_params(DIMS, mag=mag)
+    with M.Chmc(DIMS, mag=mag) as c:
+        c.set_gauge(U)
+        c.init_momentum(P)
+        H, parts = c.get_hamiltonian()
+        ho = O.hamiltonian(po, U, P)
+        assert abs(H - ho["H"]) <= 1e-12 * abs(ho["H"])
+        assert abs(parts[0] - ho["kinetic"]) <= 1e-12 * abs(ho["kinetic"])
+        c.evolve_gauge_field(0.1)
+        U1 = O.evolve_gauge(po, U, P, 0.1)
+        assert np.abs(c.get_gauge() - U1).max() < 1e-13
+        c.evolve_momentum(0.05)
+        P1 = O.evolve_momentum(DIMS, P, O.force(po, U1), 0.05)
+        assert np.abs(c.get_momentum() - P1).max() < 1e-11
+
+
+def test_reunitarize_parity():
+    U = O.gen_hot(DIMS, 12)
+    rng = np.random.default_rng(0)
+    Un = U + 1e-6 * (rng.normal(size=U.shape) + 1j * rng.normal(size=U.shape))
+    with M.Chmc(DIMS) as c:
+        c.set_gauge(Un)
+        (dev,) = c.reunitarize()
+        Ug = c.get_gauge()
+    Uo, devo = O.reunitarize(DIMS, Un)
+    assert np.abs(Ug - Uo).max() < 1e-15
+    assert abs(dev - devo) < 1e-15
+
+
+def _run_pair(dims, kw, n_traj, seed=31, start_seed=4):
+    """Trajectories on GPU (host momenta/uniforms) and oracle; returns records."""
+    po = O.make_params(dims, mag=kw.get("mag", 2), action=1 if kw.get("action", "iwasaki") == "iwasaki" else 0,
+                       beta=kw.get("beta", 2.25), n_stout=kw.get("n_stout", 0), rho=kw.get("rho", 0.1),
+                       n_steps=kw.get("n_steps", 8), tau=kw.get("tau", 1.0),
+                       accept=1 if kw.get("accept", "metropolis") == "demon" else 0, e_max=kw.get("e_max", 100.0),
+                       integrator=1 if kw.get("integrator", "fg") == "leapfrog" else 0)
+    U = O.gen_hot(dims, start_seed)
+    Uo = U.copy()
+    demon = [0.0, 0.0]
+    out = []
+    with M.Chmc(dims, seed=seed, **kw) as c:
+        c.set_gauge(U)
+        for t in range(n_traj):
+            P = O.gen_momenta(dims, seed, t)
+            u = O.gen_uniform(seed, t)
+            c.init_momentum(P)
+            c.set_uniforms([u])
+            (g,) = c.trajectory(refresh_momenta=False)
+            Uo, o = O.trajectory(po, t, Uo, P, u, demon)
+            demon = o["demon"]
+            out.append((g, o, np.abs(c.get_gauge() - Uo).max()))
+    return out
+
+
+def test_trajectory_parity_8x4_iwasaki_fp64_metropolis():
+    # the CPU-runnable configuration: 8^4, Iwasaki beta = 2.25, 8 force-gradient steps
+    res = _run_pair((8, 8, 8, 8), dict(mag=2, n_steps=8), 3)
+    for g, o, du in res:
+        assert abs(g["h_old"] - o["h_old"]) <= 1e-12 * abs(o["h_old"])
+        assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
+        assert g["accept"] == o["accept"]
+        assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-12
+        assert du < 1e-10
+
+
+def test_trajectory_parity_demon_sequence():
+    res = _run_pair((8, 8, 8, 8), dict(mag=2, n_steps=8, accept="demon", e_max=60.0), 3)
+    for g, o, _ in res:
+        assert g["accept"] == o["accept"]
+        assert abs(g["demon"][0] - o["demon"][0]) < 1e-8
+        assert abs(g["demon"][1] - o["demon"][1]) < 1e-8
+
+
+def test_trajectory_parity_three_stout_levels():
+    res = _run_pair((4, 4, 4, 8), dict(mag=2, n_stout=3, rho=0.1, n_steps=12), 2)
+    for g, o, du in res:
+        assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
+        assert g["accept"] == o["accept"]
+        assert du < 1e-10
+
+
+def test_leapfrog_parity():
+    res = _run_pair((4, 4, 4, 4), dict(mag=0, n_steps=6, integrator="leapfrog"), 1)
+    g, o, du = res[0]
+    assert abs(g["delta_h"] - o["delta_h"]) < 1e-9 and du < 1e-10
+
+
+def test_graph_run_matches_eager_trajectories():
+    dims = (4, 4, 4, 8)
+    with M.Chmc(dims, seed=41, n_stout=1, n_steps=4) as a, M.Chmc(dims, seed=41, n_stout=1, n_steps=4) as b:
+        a.hot_start(2)
+        b.hot_start(2)
+        ra = a.run_chmc(3)
+        rb = [b.trajectory(True) for _ in range(3)]
+        for x, y in zip(ra, rb):
+            assert x[0]["delta_h"] == y[0]["delta_h"] and x[0]["accept"] == y[0]["accept"]
+        assert np.array_equal(a.get_gauge(), b.get_gauge())
+
+
+def test_ensemble_chains_equal_single_lattices():
+    chains = [dict(dims=(4, 4, 4, 4), beta=2.0), dict(dims=(4, 4, 6, 6), beta=2.3), dict(dims=(6, 6, 6, 6), beta=2.6)]
+    common = dict(mag=2, n_stout=1, rho=0.1, n_steps=4, seed=100)
+    with M.Chmc(chains=chains, **common) as e:
+        e.hot_start(9)
+        re = e.run_chmc(2)
+        Ue = [e.get_gauge(k) for k in range(3)]
+    for k, ch in enumerate(chains):
+        kw = dict(common)
+        kw["seed"] = 100 + k
+        with M.Chmc(ch["dims"], beta=ch["beta"], **kw) as s:
+            # chain k of the ensemble draws its hot start from seed + k
+            s.hot_start(9 + k)
+            rs = s.run_chmc(2)
+            assert np.array_equal(s.get_gauge(), Ue[k])
+        for t in range(2):
+            assert re[t][k]["delta_h"] == rs[t][0]["delta_h"]
+
+
+def test_wilson_loops_parity():
+    U = O.gen_hot(DIMS, 14)
+    with M.Chmc(DIMS) as c:
+        c.set_gauge(U)
+        W = c.wilson_loops(3, 4)
+        for R in range(1, 4):
+            for T in range(1, 5):
+                assert abs(W[R - 1, T - 1] - O.wilson_loop(DIMS, U, (R, 0, 0), T)) < 1e-13
+        assert abs(c.avg_wilson_loop((1, 2, 0), 2) - O.wilson_loop(DIMS, U, (1, 2, 0), 2)) < 1e-13
+        c.cold_start()
+        assert np.abs(c.wilson_loops(2, 2) - 3.0).max() < 1e-14
+
+
+def test_constrained_plaquette_parity_and_invariance():
+    U = O.gen_hot((4, 4, 4, 4), 15)
+    with M.Chmc((4, 4, 4, 4), mag=2, n_steps=4, seed=3) as c:
+        c.set_gauge(U)
+        cp = c.check_constrained_plaquette()
+        assert abs(cp - O.constrained_plaquette((4, 4, 4, 4), U, 2)) < 1e-14
+        c.init_momentum(None, traj=0)
+        c.force_gradient_integrator()
+        assert abs(c.check_constrained_plaquette() - cp) < 1e-12
+
+
+def test_reversibility_fp64():
+    dims = (4, 4, 4, 8)
+    with M.Chmc(dims, mag=2, n_stout=2, n_steps=6) as c:
+        c.hot_start(3)
+        U0 = c.get_gauge()
+        c.init_momentum(None, traj=0)
+        P0 = c.get_momentum()
+        c.force_gradient_integrator()
+        c.init_momentum(-c.get_momentum())
+        c.force_gradient_integrator()
+        assert np.abs(c.get_gauge() - U0).max() < 1e-10
+        assert np.abs(c.get_momentum() + P0).max() < 1e-9
+
+
+def test_mixed_precision_force_and_trajectory():
+    dims = (4, 4, 4, 8)
+    U = O.gen_hot(dims, 16)
+    po = O.make_params(dims, mag=2, n_stout=3, rho=0.1)
+    with M.Chmc(dims, mag=2, n_stout=3, rho=0.1, precision="mixed") as c:
+        c.set_gauge(U)
+        assert maxrel(c.get_force(), O.force(po, U)) < 5e-5
+    r = {}
+    for prec in ("fp64", "mixed"):
+        with M.Chmc(dims, mag=2, n_stout=3, rho=0.1, n_steps=12, precision=prec, seed=5) as c:
+            c.set_gauge(U)
+            (r[prec],) = c.trajectory(True)
+    assert abs(r["mixed"]["h_old"] - r["fp64"]["h_old"]) <= 1e-12 * abs(r["fp64"]["h_old"])
+    assert abs(r["mixed"]["delta_h"] - r["fp64"]["delta_h"]) < 2e-2
+    assert abs(r["mixed"]["avg_plaquette"] - r["fp64"]["avg_plaquette"]) < 1e-5 or \
+        r["mixed"]["accept"] != r["fp64"]["accept"]
+
+
+def test_nan_is_reported_as_error_status():
+    U = O.gen_hot((4, 4, 4, 4), 17)
+    U[3, 1, 0, 0] = np.nan
+    with M.Chmc((4, 4, 4, 4), n_steps=2) as c:
+        c.set_gauge(U)
+        with pytest.raises(M.MagError) as e:
+            c.trajectory(True)
+        assert e.value.code == -3
