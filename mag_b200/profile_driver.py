@@ -1,0 +1,40 @@
+"""Run force evaluations of one lattice for profiling (e.g. under ncu).
+
+    python -m mag_b200.profile_driver --dims 24 24 24 24 --n-stout 3 --precision fp64 --reps 2
+
+Creates one context, draws a Philox hot start, then times `reps` force
+evaluations (plus one warm-up evaluation) and the named single kernels, and
+prints the CUDA-event times.  Every launch uses live data, so a profiler that
+selects any of them sees a representative kernel.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import mag_b200 as M
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--dims", type=int, nargs=4, default=[24, 24, 24, 24])
+    ap.add_argument("--n-stout", type=int, default=3)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--action", default="iwasaki", choices=["iwasaki", "wilson"])
+    ap.add_argument("--mag", type=int, default=2)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--kernels", nargs="*", default=[])
+    a = ap.parse_args(argv)
+    with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1,
+                precision=a.precision, seed=1) as c:
+        c.hot_start(1)
+        out = {"dims": a.dims, "precision": a.precision, "n_stout": a.n_stout,
+               "force_eval_ms": c.time_force(a.reps)}
+        for k in a.kernels:
+            out[f"{k}_ms"] = c.time_kernel(k, a.reps)
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,35 @@
+// C++ driver in the style of quench_test/main.C: constrained Iwasaki HMC on a
+// hot start through include/mag_field.hpp; prints one JSON line.
+#include <cstdio>
+#include <cstdlib>
+
+#include "mag_field.hpp"
+
+int main(int argc, char** argv) {
+    const int L = argc > 1 ? std::atoi(argv[1]) : 4;
+    mag_b200::Arg_chmc arg;
+    arg.mag = 2;
+    arg.trajectory_length = 4;
+    arg.num_trajectory = 3;
+    arg.beta = 2.25;
+    arg.dt = 1.0 / arg.trajectory_length;
+    mag_b200::Options opt;
+    opt.n_stout = 1;
+    opt.seed = 5;
+    try {
+        mag_b200::Lattice lat({L, L, L, 2 * L}, arg, opt);
+        lat.hot_start(3);
+        const double c0 = mag_b200::check_constrained_plaquette(lat);
+        std::vector<double> part;
+        const double h = mag_b200::get_hamiltonian(lat, part);
+        auto res = mag_b200::run_chmc(lat, stderr);
+        const double c1 = mag_b200::check_constrained_plaquette(lat);
+        std::printf("{\"h0\": %.17g, \"kin0\": %.17g, \"dh\": [%.17g, %.17g, %.17g], \"plaq\": %.17g, "
+                    "\"cplaq_before\": %.17g, \"cplaq_after\": %.17g}\n",
+                    h, part[0], res[0].delta_h, res[1].delta_h, res[2].delta_h, mag_b200::avg_plaquette(lat), c0, c1);
+    } catch (const mag_b200::Error& e) {
+        std::fprintf(stderr, "error %d: %s\n", e.code, e.what());
+        return 2;
+    }
+    return 0;
+}
