@@ -152,6 +152,25 @@ int mag_wilson_loops(mag_ctx* ctx, int chain, int Rmax, int Tmax, double* out);
 /* check_constrained_plaquette (field-matrix.h:407-443) */
 int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out);
 
+/* ------------------------------------------------------- allocation-free */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+   (a driver that hands this library memory from a device pool it manages
+   itself, or a loop that must not pay for cudaMalloc's implicit device
+   synchronisation): the plaquette and rectangle sums of total_plaq /
+   total_rectangular (field-matrix.h:299-385), d_sums[0] = sum ReTr plaquette,
+   d_sums[1] = sum ReTr rectangle, from links already in device memory in the
+   AoS layout double[V][4][3][3][2].  Both pointers are device memory owned by
+   the caller; the call only enqueues work on `stream` (a cudaStream_t, NULL =
+   default stream) and returns.  It allocates nothing: its block partials live
+   in one static device array of MAG_NOALLOC_MAX_SITES / 256 * 2 double-double
+   entries (2 MiB), held by every GPU that loads the library until exit, and
+   lattices larger than MAG_NOALLOC_MAX_SITES sites are rejected with
+   MAG_ERR_ARG.  The first call on a device looks up that array's address;
+   make that first call before any stream capture.  Calls share the array, so
+   calls that overlap on the GPU race with each other. */
+#define MAG_NOALLOC_MAX_SITES (1 << 24)
+int mag_action_sums_noalloc(const int dims[4], const double* d_links, double* d_sums, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,6 +110,7 @@ SIGNATURES = {
     "mag_time_force": [_CTX, ctypes.c_int, _DP],
     "mag_time_kernel": [_CTX, ctypes.c_char_p, ctypes.c_int, _DP],
     "mag_graph_kernel_count": [_CTX, _IP],
+    "mag_action_sums_noalloc": [_IP, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "mag_probe_fma_peak": [ctypes.c_int, _DP],
 }
 _RESTYPE = {"mag_last_error": ctypes.c_char_p}

@@ -75,6 +75,11 @@ hdd h_neg(hdd a) { return hdd{-a.hi, -a.lo}; }
 
 }  // namespace
 
+namespace magb {
+// lets the allocation-free entry point (noalloc.cu) report through mag_last_error()
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace magb
+
 struct mag_ctx {
     mag_params p{};
     std::vector<mag_params> cp;
