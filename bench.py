@@ -3,16 +3,18 @@
 
 A step is one HMC trajectory of the workload (momentum refresh, H_old, the
 force-gradient molecular dynamics, reunitarisation, H_new, accept/reject),
-replayed as one CUDA graph.  The default workload is the 16^3 x 32 lattice,
-Iwasaki beta = 2.25 (c1 = -0.331), three stout levels rho = 0.1, twelve
-force-gradient steps of tau = 1, constraint magnification 2, Metropolis accept,
-plain FP64; the same lattice in mixed precision is measured beside it.
+replayed as one CUDA graph; for the ensemble workload a step advances every
+chain by one trajectory and `value` counts chain-trajectories.  The default
+workload is the 16^3 x 32 lattice, Iwasaki beta = 2.25 (c1 = -0.331), three
+stout levels rho = 0.1, twelve force-gradient steps of tau = 1, constraint
+magnification 2, Metropolis accept, plain FP64; the same lattice in mixed
+precision is measured beside it.
 
   python bench.py [--gpus N --steps K --warmup W] [--workload NAME] [--impl reference]
 
 With --gpus N > 1 (launched by torchrun) every rank advances its own
-independent chain on its own GPU: replicas, weak scaling, no collective in the
-data path (the only collective is the max over ranks of the timing).
+independent chain(s) on its own GPU: replicas, weak scaling, no collective in
+the data path (the only collective is the max over ranks of the timing).
 
 --impl reference times the reference's algorithm on the host cores: the
 reference itself cannot be built here (it needs CPS, Qlattice, QMP, MPI), so
@@ -34,15 +36,28 @@ sys.path.insert(0, ROOT)
 
 METRIC = "HMC traj/s & force site-updates/s, mixed vs FP64 GPU at equal ΔH/plaquette"
 
+
+def ensemble_chains(seed: int = 4):
+    """96 independent chains: 48 x 8^4, 32 x 12^4, 16 x 16^4, beta uniform in [2.0, 2.6) from seed."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    dims = [(8,) * 4] * 48 + [(12,) * 4] * 32 + [(16,) * 4] * 16
+    return [dict(dims=d, beta=float(b)) for d, b in zip(dims, rng.uniform(2.0, 2.6, len(dims)))]
+
+
 WORKLOADS = {
     # 16^3 x 32, 3 stout levels, 12 FG steps, FP64 (the FP64 GPU path checked against the CPU oracle)
     "16x16x16x32_iwasaki_3stout": dict(dims=(16, 16, 16, 32), beta=2.25, n_stout=3, n_steps=12, precision="fp64"),
-    # 32^4, 3 stout levels, 16 FG steps (mixed precision target beside FP64)
+    # 32^4, 3 stout levels, 16 FG steps: FP64 with the mixed-precision leg beside it
     "32x32x32x32_iwasaki_3stout": dict(dims=(32, 32, 32, 32), beta=2.25, n_stout=3, n_steps=16, precision="fp64"),
     # 8^4 thin-link Iwasaki, 8 FG steps (the CPU-runnable configuration)
     "8x8x8x8_iwasaki_thin": dict(dims=(8, 8, 8, 8), beta=2.25, n_stout=0, n_steps=8, precision="fp64"),
-    # 48^3 x 96, beta 2.37, 3 stout levels, 16 FG steps
-    "48x48x48x96_iwasaki_3stout": dict(dims=(48, 48, 48, 96), beta=2.37, n_stout=3, n_steps=16, precision="mixed"),
+    # 96 chains in one context, 1 stout level, 8 FG steps, mixed precision
+    "ensemble_96chains": dict(chains="ensemble", n_stout=1, n_steps=8, precision="mixed"),
+    # 48^3 x 96, beta 2.37, 3 stout levels, 16 FG steps, mixed, Wilson loops R, T <= 8 after each trajectory
+    "48x48x48x96_iwasaki_3stout_wloops": dict(dims=(48, 48, 48, 96), beta=2.37, n_stout=3, n_steps=16,
+                                             precision="mixed", wilson=8),
 }
 DEFAULT = "16x16x16x32_iwasaki_3stout"
 COMMON = dict(mag=2, action="iwasaki", c1=-0.331, rho=0.1, tau=1.0, accept="metropolis", integrator="fg")
@@ -79,6 +94,8 @@ def parse():
 def workload_params(name: str) -> dict:
     p = dict(COMMON)
     p.update(WORKLOADS[name])
+    if p.get("chains") == "ensemble":
+        p["chains"] = ensemble_chains()
     return p
 
 
@@ -87,6 +104,27 @@ def site_count(dims) -> int:
     for d in dims:
         v *= d
     return v
+
+
+def total_sites(params) -> int:
+    if "chains" in params:
+        return sum(site_count(c["dims"]) for c in params["chains"])
+    return site_count(params["dims"])
+
+
+def max_over_ranks(x: float, dist, device: str) -> float:
+    """Max of a per-rank scalar over the process group (identity without one)."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_seed(rank: int) -> int:
+    return 1000 + 7919 * rank
 
 
 # ---------------------------------------------------------------- clocks
@@ -151,17 +189,22 @@ def gpu_index_for_smi() -> str:
 
 
 # ---------------------------------------------------------------- CPU legs
-def cpu_sample(params: dict) -> dict:
-    """Time the oracle (FP64, OpenMP) on one force evaluation, one link update
-    and one Hamiltonian evaluation of the full workload; extrapolate to a
-    trajectory: 4n forces + (4n+1) link updates + 2 Hamiltonians."""
-    import numpy as np
-
+def oracle_params(params):
     import oracle as O
 
-    dims = params["dims"]
-    po = O.make_params(dims, mag=params["mag"], action=1, beta=params["beta"], c1=params["c1"], rho=params["rho"],
-                       n_stout=params["n_stout"], tau=params["tau"], n_steps=params["n_steps"])
+    dims = params["dims"] if "dims" in params else params["chains"][-1]["dims"]
+    beta = params.get("beta", params["chains"][-1]["beta"] if "chains" in params else 2.25)
+    return dims, O.make_params(dims, mag=params["mag"], action=1, beta=beta, c1=params["c1"], rho=params["rho"],
+                               n_stout=params["n_stout"], tau=params["tau"], n_steps=params["n_steps"])
+
+
+def cpu_sample(params: dict) -> dict:
+    """Time the oracle (FP64, OpenMP) on one force evaluation, one link update
+    and one Hamiltonian evaluation of the full lattice; extrapolate to a
+    trajectory: 4n forces + (4n+1) link updates + 2 Hamiltonians."""
+    import oracle as O
+
+    dims, po = oracle_params(params)
     U = O.gen_hot(dims, 1)
     P = O.gen_momenta(dims, 1, 0)
     t0 = time.perf_counter()
@@ -175,7 +218,6 @@ def cpu_sample(params: dict) -> dict:
     t_ham = time.perf_counter() - t0
     n = params["n_steps"]
     traj_s = 4 * n * t_force + (4 * n + 1) * t_evolve + 2 * t_ham
-    del np
     return {"t_force": t_force, "t_evolve": t_evolve, "t_ham": t_ham, "traj_s": traj_s,
             "cores": O.lib().mo_get_threads()}
 
@@ -185,9 +227,7 @@ def reference_arm(args, params, rank: int, world: int):
         return
     import oracle as O
 
-    dims = params["dims"]
-    po = O.make_params(dims, mag=params["mag"], action=1, beta=params["beta"], c1=params["c1"], rho=params["rho"],
-                       n_stout=params["n_stout"], tau=params["tau"], n_steps=params["n_steps"])
+    dims, po = oracle_params(params)
     U = O.gen_hot(dims, 1)
     P = O.gen_momenta(dims, 1, 0)
     t0 = time.perf_counter()
@@ -206,12 +246,16 @@ def reference_arm(args, params, rank: int, world: int):
     t_force = statistics.median(ts)
     n = params["n_steps"]
     traj_s = 4 * n * t_force + (4 * n + 1) * t_evolve + 2 * t_ham
-    value = 1.0 / traj_s
-    sample = (f"each step = one {params['n_stout']}-level stout Iwasaki force evaluation of the full lattice "
-              f"(FP64 oracle port); trajectory = {4 * n} force evals + {4 * n + 1} link updates + 2 Hamiltonians")
+    nchain = len(params["chains"]) if "chains" in params else 1
+    # ensemble: every chain's trajectory costs (its volume / the sampled volume) of the sampled one
+    traj_s_job = traj_s * total_sites(params) / site_count(dims)
+    value = nchain / traj_s_job
+    sample = (f"each step = one {params['n_stout']}-level stout Iwasaki force evaluation of a "
+              f"{'x'.join(map(str, dims))} lattice (FP64 oracle port); trajectory = {4 * n} force evals + "
+              f"{4 * n + 1} link updates + 2 Hamiltonians" + (", scaled by volume to all chains" if nchain > 1 else ""))
     line = {
         "metric": METRIC, "value": value, "unit": "traj/s", "impl": "reference", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": traj_s * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": traj_s_job * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
         "config": config_of(args.workload, params, world),
         "cpu_baseline": {"value": value, "unit": "traj/s", "cores": O.lib().mo_get_threads(), "kind": "port",
@@ -224,14 +268,31 @@ def reference_arm(args, params, rank: int, world: int):
 
 
 def config_of(name, params, world):
-    return {"workload": name, "lattice": "x".join(str(d) for d in params["dims"]), "action": "iwasaki",
-            "beta": params["beta"], "c1": params["c1"], "stout_levels": params["n_stout"], "rho": params["rho"],
-            "fg_steps": params["n_steps"], "tau": params["tau"], "mag": params["mag"],
-            "precision": params["precision"], "accept": "metropolis", "parallelism": f"replicas{world}",
-            "l2": "working set > 126 MB L2 (links, momenta, stout levels)"}
+    c = {"workload": name, "action": "iwasaki", "c1": params["c1"], "stout_levels": params["n_stout"],
+         "rho": params["rho"], "fg_steps": params["n_steps"], "tau": params["tau"], "mag": params["mag"],
+         "precision": params["precision"], "accept": "metropolis", "parallelism": f"replicas{world}",
+         "l2": "working set > 126 MB L2 (links, momenta, stout levels)"}
+    if "chains" in params:
+        c["chains"] = "48x8^4 + 32x12^4 + 16x16^4, beta ~ U[2.0, 2.6) per chain"
+        c["sites"] = total_sites(params)
+    else:
+        c["lattice"] = "x".join(str(d) for d in params["dims"])
+        c["beta"] = params["beta"]
+    if params.get("wilson"):
+        c["wilson_loops"] = f"R, T <= {params['wilson']} after each trajectory (FP64)"
+    return c
 
 
 # ---------------------------------------------------------------- GPU arm
+def make_ctx(M, params, seed, precision, n_forced):
+    kw = {k: v for k, v in params.items() if k not in ("dims", "chains", "wilson")}
+    kw["precision"] = precision
+    kw["n_forced_accept"] = n_forced  # the reference forces the first accepts (field-hmc.h:826)
+    if "chains" in params:
+        return M.Chmc(chains=params["chains"], seed=seed, **kw)
+    return M.Chmc(params["dims"], seed=seed, **kw)
+
+
 def run_gpu(args, params, rank, world, dist):
     import numpy as np
     import torch
@@ -239,17 +300,14 @@ def run_gpu(args, params, rank, world, dist):
     import mag_b200 as M
     from mag_b200.field_hmc import probe_fma_peak
 
-    dims = params["dims"]
-    V = site_count(dims)
+    V = total_sites(params)
     n = params["n_steps"]
-    seed = 1000 + 7919 * rank
-    kw = {k: v for k, v in params.items() if k != "dims"}
+    nchain = len(params["chains"]) if "chains" in params else 1
+    seed = rank_seed(rank)
+    wl = params.get("wilson", 0)
 
     def timed_run(prec: str):
-        kk = dict(kw)
-        kk["precision"] = prec
-        kk["n_forced_accept"] = args.warmup  # the reference forces the first accepts (field-hmc.h:826)
-        c = M.Chmc(dims, seed=seed, **kk)
+        c = make_ctx(M, params, seed, prec, args.warmup)
         c.hot_start(seed)
         if args.warmup:
             c.run_chmc(args.warmup)
@@ -261,23 +319,28 @@ def run_gpu(args, params, rank, world, dist):
         if sampler:
             sampler.start()
             time.sleep(0.3)
-        recs = c.run_chmc(args.steps)
+        recs, ms, wl_ms = [], 0.0, 0.0
+        if wl:
+            for _ in range(args.steps):
+                recs += c.run_chmc(1)
+                ms += c.last_run_ms()
+                c.wilson_loops(wl, wl)
+                wl_ms += c.last_measure_ms()
+        else:
+            recs = c.run_chmc(args.steps)
+            ms = c.last_run_ms()
         torch.cuda.synchronize()
         clocks = sampler.stop() if sampler else None
-        ms = c.last_run_ms()
-        if dist:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return c, recs, ms, clocks
+        total = max_over_ranks(ms + wl_ms, dist, "cuda")
+        return c, recs, total, wl_ms, clocks
 
-    c64, rec64, ms64, clocks = timed_run(params["precision"])
     head_prec = params["precision"]
-    value = world * args.steps / (ms64 / 1e3)
+    c64, rec64, ms64, wl_ms, clocks = timed_run(head_prec)
+    value = world * nchain * args.steps / (ms64 / 1e3)
     ms_per_step = ms64 / args.steps
-    dh = [r[0]["delta_h"] for r in rec64]
-    acc = [r[0]["accept"] for r in rec64]
-    plaq = [r[0]["avg_plaquette"] for r in rec64]
+    dh = [r[k]["delta_h"] for r in rec64 for k in range(nchain)]
+    acc = [r[k]["accept"] for r in rec64 for k in range(nchain)]
+    plaq = rec64[-1][0]["avg_plaquette"]
     kernels_per_traj = c64.graph_kernel_count()
 
     # dominant kernel and its roofline (device-timed on the launching stream)
@@ -294,16 +357,14 @@ def run_gpu(args, params, rank, world, dist):
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath):
-        tj = json.load(open(tpath))
-        traffic = tj.get(f"{args.workload}:{head_prec}:{dom}")
+        traffic = json.load(open(tpath)).get(f"{args.workload}:{head_prec}:{dom}")
     roofline = {"bound": prec_key, "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "peak_source": f"measured CUDA-core {prec_key.upper()} FMA throughput (mag_probe_fma_peak)",
                 "flops_per_site": FLOPS_PER_SITE[dom], "launch_ms": kt[dom],
-                "kernel_ms": kt, "force_eval_ms": t_force_eval}
-    # HBM roofline of the streaming link update
+                "kernel_ms": kt, "force_eval_ms": t_force_eval, "tuned_min_blocks": c64.autotune(3)}
     ev_ms = c64.time_kernel("evolve", 5)
-    bytes_evolve = V * 4 * (144 + 144 + 64)  # read U, write U, read P (FP64 master update)
+    bytes_evolve = V * 4 * (144 + 144 + 64) + (V * 4 * 72 if head_prec == "mixed" else 0)
     peaks = {}
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
@@ -311,21 +372,25 @@ def run_gpu(args, params, rank, world, dist):
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     roofline["evolve_hbm"] = {"achieved": bytes_evolve / (ev_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                               "frac": bytes_evolve / (ev_ms * 1e-3) / 1e9 / hbm_peak,
-                              "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback"}
+                              "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
+                                              else "fallback 6.65 TB/s")}
 
-    # end to end through the public API with pinned host buffers
+    # end to end through the public API with pinned host buffers (chain 0)
     e2e = None
-    if args.e2e_steps > 0:
-        field_bytes = V * 4 * 9 * 16
-        Uh = torch.empty(V * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(V, 4, 3, 3)
-        Ph = torch.empty(V * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(V, 4, 3, 3)
+    if args.e2e_steps > 0 and nchain == 1:
+        V0 = c64.volume(0)
+        field_bytes = V0 * 4 * 9 * 16
+        Uh = torch.empty(V0 * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(V0, 4,
+                                                                                                            3, 3)
+        Ph = torch.empty(V0 * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(V0, 4,
+                                                                                                            3, 3)
         Uh[:] = c64.get_gauge()
         rng = np.random.default_rng(seed)
         Ps = []
+        s2, s6 = 1 / np.sqrt(2), 1 / np.sqrt(6)
         for _ in range(args.e2e_steps):
-            xi = rng.standard_normal((V, 4, 8))
-            P = np.zeros((V, 4, 3, 3), np.complex128)
-            s2, s6 = 1 / np.sqrt(2), 1 / np.sqrt(6)
+            xi = rng.standard_normal((V0, 4, 8))
+            P = np.zeros((V0, 4, 3, 3), np.complex128)
             P[..., 0, 1] = (xi[..., 0] - 1j * xi[..., 1]) * s2
             P[..., 0, 2] = (xi[..., 3] - 1j * xi[..., 4]) * s2
             P[..., 1, 2] = (xi[..., 5] - 1j * xi[..., 6]) * s2
@@ -344,13 +409,11 @@ def run_gpu(args, params, rank, world, dist):
             c64.init_momentum(Ph)
             c64.set_uniforms([0.5])
             c64.trajectory(refresh_momenta=False)
+            if wl:
+                c64.wilson_loops(wl, wl)
             Uh[:] = c64.get_gauge()
         torch.cuda.synchronize()
-        el = time.perf_counter() - t0
-        if dist:
-            t = torch.tensor([el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            el = float(t.item())
+        el = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
         e2e = {"value": world * args.e2e_steps / el, "unit": "traj/s", "h2d_bytes_per_step": 2 * field_bytes + 8,
                "d2h_bytes_per_step": field_bytes + 152, "steps": args.e2e_steps,
                "path": "mag_gauge_set + mag_momentum_set + mag_uniforms_set + mag_trajectory + mag_gauge_get"}
@@ -358,8 +421,8 @@ def run_gpu(args, params, rank, world, dist):
 
     mixed = None
     if not args.no_mixed and head_prec == "fp64":
-        cm, recm, msm, _ = timed_run("mixed")
-        vm = world * args.steps / (msm / 1e3)
+        cm, recm, msm, _, _ = timed_run("mixed")
+        vm = world * nchain * args.steps / (msm / 1e3)
         mixed = {"value": vm, "unit": "traj/s", "ms_per_step": msm / args.steps, "speedup_vs_fp64": vm / value,
                  "delta_h_mean": statistics.fmean(r[0]["delta_h"] for r in recm),
                  "acceptance": statistics.fmean(r[0]["accept"] for r in recm),
@@ -370,10 +433,13 @@ def run_gpu(args, params, rank, world, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         s = cpu_sample(params)
-        cpu = {"value": 1.0 / s["traj_s"], "unit": "traj/s", "cores": s["cores"], "kind": "port",
+        vol_ratio = V / site_count(oracle_params(params)[0])
+        cpu = {"value": nchain / (s["traj_s"] * vol_ratio), "unit": "traj/s", "cores": s["cores"], "kind": "port",
                "sample": (f"oracle FP64 port, OpenMP: one force evaluation ({s['t_force']:.2f} s), one link update "
-                          f"({s['t_evolve']:.2f} s) and one Hamiltonian ({s['t_ham']:.2f} s) of the full lattice, "
-                          f"extrapolated to {4 * n} force evals + {4 * n + 1} updates + 2 Hamiltonians per trajectory"),
+                          f"({s['t_evolve']:.2f} s) and one Hamiltonian ({s['t_ham']:.2f} s) of the "
+                          f"{'x'.join(map(str, oracle_params(params)[0]))} lattice, extrapolated to {4 * n} force "
+                          f"evals + {4 * n + 1} updates + 2 Hamiltonians per trajectory"
+                          + (" and by volume to all chains" if nchain > 1 else "")),
                "force_evals_per_s": 1.0 / s["t_force"]}
 
     if rank != 0:
@@ -384,13 +450,15 @@ def run_gpu(args, params, rank, world, dist):
         "vs_baseline": None, "dtype": "f64" if head_prec == "fp64" else "f32+f64",
         "data": "synthetic: Philox Haar-random hot start, Gaussian momenta, Philox Metropolis uniforms",
         "config": config_of(args.workload, params, world),
-        "force_evals_per_s": world * 4 * n * args.steps / (ms64 / 1e3),
+        "force_evals_per_s": world * nchain * 4 * n * args.steps / (ms64 / 1e3),
         "site_updates_per_s": world * V * 4 * n * args.steps / (ms64 / 1e3),
         "delta_h_mean": statistics.fmean(dh), "delta_h_abs_mean": statistics.fmean(abs(x) for x in dh),
-        "acceptance": statistics.fmean(acc), "plaquette": plaq[-1],
+        "acceptance": statistics.fmean(acc), "plaquette": plaq,
         "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": kernels_per_traj * args.steps,
     }
+    if wl:
+        line["wilson_loops_ms_per_step"] = wl_ms / args.steps
     print(json.dumps(line), flush=True)
 
 

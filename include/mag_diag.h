@@ -16,6 +16,8 @@ extern "C" {
 
 /* device time of the trajectories of the last mag_run call (ms) */
 int mag_last_run_ms(mag_ctx* ctx, double* total_ms);
+/* device time of the kernels of the last mag_wilson_loops call (ms) */
+int mag_last_measure_ms(mag_ctx* ctx, double* ms);
 /* average device time of one force evaluation (thin or smeared, in the
    context's precision, constraint fix-up included) on the current links */
 int mag_time_force(mag_ctx* ctx, int reps, double* ms_per_eval);
@@ -23,10 +25,16 @@ int mag_time_force(mag_ctx* ctx, int reps, double* ms_per_eval);
    fields: "force", "staple", "stout_forward", "stout_lambda", "stout_chain",
    "evolve", "kick", "action" */
 int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms_per_launch);
+/* re-run the launch-configuration tuner: time every register-cap variant of the
+   staple / force / stout kernels on the live fields (`reps` launches each) and
+   keep the fastest; report (may be NULL) receives a JSON object
+   {"family": [min blocks per SM for FP64, for FP32], ...}.  The first
+   trajectory, integration or graph build of a context runs the tuner once. */
+int mag_autotune(mag_ctx* ctx, int reps, char* report, size_t len);
 /* number of kernel nodes in the captured trajectory graph (building it if needed) */
 int mag_graph_kernel_count(mag_ctx* ctx, int* kernels);
-/* measured CUDA-core FMA throughput of this device: precision 0 = FP64,
-   1 = FP32; tflops counts 2 flops per FMA */
+/* measured CUDA-core FMA throughput of this device: precision 0 = FP64 FMA,
+   1 = FP32 FMA, 2 = packed FP32 FMA (fma.rn.f32x2); tflops counts 2 flops per FMA */
 int mag_probe_fma_peak(int precision, double* tflops);
 
 #ifdef __cplusplus

@@ -107,9 +107,11 @@ SIGNATURES = {
     "mag_wilson_loops": [_CTX, ctypes.c_int, ctypes.c_int, ctypes.c_int, _DP],
     "mag_constrained_plaquette": [_CTX, ctypes.c_int, _DP],
     "mag_last_run_ms": [_CTX, _DP],
+    "mag_last_measure_ms": [_CTX, _DP],
     "mag_time_force": [_CTX, ctypes.c_int, _DP],
     "mag_time_kernel": [_CTX, ctypes.c_char_p, ctypes.c_int, _DP],
     "mag_graph_kernel_count": [_CTX, _IP],
+    "mag_autotune": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t],
     "mag_action_sums_noalloc": [_IP, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "mag_probe_fma_peak": [ctypes.c_int, _DP],
 }

@@ -58,23 +58,29 @@ struct AcceptArgs {
 };
 
 // ---- force and staples (kernels_force.cu)
+// `v` selects the register-cap variant 0..3 (minimum 2..5 resident 128-thread
+// blocks per SM, i.e. at most 255 / 168 / 128 / 102 registers per thread).
+constexpr int kNumVariants = 4;
+enum KernelFamily { KF_FORCE = 0, KF_STAPLE, KF_STOUT_FWD, KF_STOUT_LAMBDA, KF_STOUT_CHAIN, KF_COUNT };
+
 template <typename T>
-void launch_force(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, bool iwasaki, cudaStream_t s);
+void launch_force(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, bool iwasaki, int v, cudaStream_t s);
 template <typename T>
-void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> Z, bool iwasaki, cudaStream_t s);
+void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> Z, bool iwasaki, int v, cudaStream_t s);
 template <typename T>
 void launch_constraint_fixup(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, cudaStream_t s);
 template <typename T>
-void launch_stout_forward(const DevGeom& g, LinkPlanes<T> Uin, LinkPlanes<T> Uout, AlgPlanes<T> Q, cudaStream_t s);
+void launch_stout_forward(const DevGeom& g, LinkPlanes<T> Uin, LinkPlanes<T> Uout, AlgPlanes<T> Q, int v,
+                          cudaStream_t s);
 template <typename T>
 void launch_stout_lambda(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Q, LinkPlanes<T> Z, AlgPlanes<T> Lam,
-                         LinkPlanes<T> Zp, cudaStream_t s);
+                         LinkPlanes<T> Zp, int v, cudaStream_t s);
 template <typename T>
 void launch_stout_chain(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Lam, LinkPlanes<T> Zp, LinkPlanes<T> Zout,
-                        cudaStream_t s);
+                        int v, cudaStream_t s);
 template <typename T>
 void launch_stout_chain_force(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> Lam, LinkPlanes<T> Zp, AlgPlanes<T> F,
-                              cudaStream_t s);
+                              int v, cudaStream_t s);
 
 // ---- streaming kernels (kernels_update.cu)
 template <typename TU, typename TX>
@@ -120,6 +126,8 @@ void launch_links_to_aos_t(LinkPlanes<T> U, int chain_off, int V, double* aos, c
 // ---- FMA throughput probe: nblocks x 256 threads, 8 x iters FMAs each
 template <typename T>
 void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s);
+// packed FP32 (fma.rn.f32x2): out holds nblocks * 256 float2
+void launch_ffma2_probe(void* out, int nblocks, int iters, cudaStream_t s);
 
 // ---- measurements (kernels_wloop.cu)
 // planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;

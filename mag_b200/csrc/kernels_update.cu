@@ -423,11 +423,30 @@ __global__ void k_fma_probe(T* out, int iters, T b, T c) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// packed FP32 probe: eight independent fma.rn.f32x2 chains per thread
+__global__ void k_ffma2_probe(float2* out, int iters) {
+    float2 a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = make_float2((float)(threadIdx.x + k) * 1e-3f, (float)k * 1e-3f);
+    const float2 b = make_float2(0.999999f, 0.999998f), c = make_float2(1e-6f, 2e-6f);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = __ffma2_rn(a[k], b, c);
+    }
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 8; k++) s = __fadd2_rn(s, a[k]);
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
 
 template <typename T>
 void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s) {
     k_fma_probe<T><<<nblocks, kBlock, 0, s>>>(out, iters, (T)0.999999, (T)1e-6);
+}
+void launch_ffma2_probe(void* out, int nblocks, int iters, cudaStream_t s) {
+    k_ffma2_probe<<<nblocks, kBlock, 0, s>>>(static_cast<float2*>(out), iters);
 }
 template void launch_fma_probe<float>(float*, int, int, cudaStream_t);
 template void launch_fma_probe<double>(double*, int, int, cudaStream_t);

@@ -118,6 +118,7 @@ struct mag_ctx {
     int graph_kernels = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_run_ms = 0.0;
+    double last_measure_ms = 0.0;
 
     ~mag_ctx() { release(); }
 
@@ -271,22 +272,30 @@ struct mag_ctx {
     }
 
     // ----------------------------------------------------------- force
+    // register-cap variant per kernel family and precision ([0] double, [1] float)
+    int tune[KF_COUNT][2] = {};
+    bool tuned = false;
+    template <typename T>
+    int var(KernelFamily f) const {
+        return tune[f][sizeof(T) == 8 ? 0 : 1];
+    }
+
     template <typename T>
     void force_eval(LinkPlanes<T> Uin, AlgPlanes<T> Fout, StoutBufs<T>& b) {
         if (p.n_stout == 0) {
-            launch_force<T>(geom, Uin, Fout, iwasaki, stream);
+            launch_force<T>(geom, Uin, Fout, iwasaki, var<T>(KF_FORCE), stream);
         } else {
             LinkPlanes<T> cur = Uin;
             for (int k = 0; k < p.n_stout; k++) {
-                launch_stout_forward<T>(geom, cur, b.lv[k], b.Q[k], stream);
+                launch_stout_forward<T>(geom, cur, b.lv[k], b.Q[k], var<T>(KF_STOUT_FWD), stream);
                 cur = b.lv[k];
             }
-            launch_staple_dagger<T>(geom, cur, b.za, iwasaki, stream);
+            launch_staple_dagger<T>(geom, cur, b.za, iwasaki, var<T>(KF_STAPLE), stream);
             for (int k = p.n_stout - 1; k >= 0; k--) {
                 LinkPlanes<T> ul = k == 0 ? Uin : b.lv[k - 1];
-                launch_stout_lambda<T>(geom, ul, b.Q[k], b.za, b.lam, b.zp, stream);
-                if (k == 0) launch_stout_chain_force<T>(geom, ul, b.lam, b.zp, Fout, stream);
-                else launch_stout_chain<T>(geom, ul, b.lam, b.zp, b.za, stream);
+                launch_stout_lambda<T>(geom, ul, b.Q[k], b.za, b.lam, b.zp, var<T>(KF_STOUT_LAMBDA), stream);
+                if (k == 0) launch_stout_chain_force<T>(geom, ul, b.lam, b.zp, Fout, var<T>(KF_STOUT_CHAIN), stream);
+                else launch_stout_chain<T>(geom, ul, b.lam, b.zp, b.za, var<T>(KF_STOUT_CHAIN), stream);
             }
         }
         if (any_mag) launch_constraint_fixup<T>(geom, Uin, Fout, stream);
@@ -296,11 +305,90 @@ struct mag_ctx {
     LinkPlanes<double> smear64() {
         LinkPlanes<double> cur = U;
         for (int k = 0; k < p.n_stout; k++) {
-            launch_stout_forward<double>(geom, cur, st64.lv[k], st64.Q[k], stream);
+            launch_stout_forward<double>(geom, cur, st64.lv[k], st64.Q[k], var<double>(KF_STOUT_FWD), stream);
             cur = st64.lv[k];
         }
         return cur;
     }
+
+    // one launch of a kernel family on the live buffers of precision T
+    template <typename T>
+    void launch_one(KernelFamily f, int v, StoutBufs<T>& b, LinkPlanes<T> Uin, AlgPlanes<T> Fo, LinkPlanes<T> zs) {
+        const int L = p.n_stout;
+        switch (f) {
+            case KF_FORCE: launch_force<T>(geom, Uin, Fo, iwasaki, v, stream); break;
+            case KF_STAPLE:
+                launch_staple_dagger<T>(geom, L ? b.lv[L - 1] : Uin, L ? b.za : zs, iwasaki, v, stream);
+                break;
+            case KF_STOUT_FWD: launch_stout_forward<T>(geom, Uin, b.lv[0], b.Q[0], v, stream); break;
+            case KF_STOUT_LAMBDA: launch_stout_lambda<T>(geom, Uin, b.Q[0], b.za, b.lam, b.zp, v, stream); break;
+            case KF_STOUT_CHAIN: launch_stout_chain<T>(geom, Uin, b.lam, b.zp, b.za, v, stream); break;
+            default: break;
+        }
+    }
+
+    template <typename T>
+    int time_one(KernelFamily f, int v, int reps, StoutBufs<T>& b, LinkPlanes<T> Uin, AlgPlanes<T> Fo,
+                 LinkPlanes<T> zs, double* ms) {
+        launch_one<T>(f, v, b, Uin, Fo, zs);
+        MAG_CUDA(cudaEventRecord(ev0, stream));
+        for (int i = 0; i < reps; i++) launch_one<T>(f, v, b, Uin, Fo, zs);
+        MAG_CUDA(cudaEventRecord(ev1, stream));
+        MAG_TRY(sync("time kernel"));
+        float t = 0.f;
+        MAG_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+        *ms = t / reps;
+        return MAG_OK;
+    }
+
+    // The tuner: time every register-cap variant of every kernel family the
+    // integrator uses, on live data, and keep the fastest.  Variants compute
+    // identical results (same instructions, different register allocation).
+    template <typename T>
+    int tune_precision(int reps, StoutBufs<T>& b, LinkPlanes<T> Uin, AlgPlanes<T> Fo, LinkPlanes<T> zs) {
+        force_eval<T>(Uin, Fo, b);
+        std::vector<KernelFamily> fams;
+        if (p.n_stout == 0) fams = {KF_FORCE};
+        else fams = {KF_STAPLE, KF_STOUT_FWD, KF_STOUT_LAMBDA, KF_STOUT_CHAIN};
+        for (KernelFamily f : fams) {
+            double best = 1e300;
+            int bv = 0;
+            for (int v = 0; v < kNumVariants; v++) {
+                double ms = 0.0;
+                MAG_TRY(time_one<T>(f, v, reps, b, Uin, Fo, zs, &ms));
+                if (ms < best) {
+                    best = ms;
+                    bv = v;
+                }
+            }
+            tune[f][sizeof(T) == 8 ? 0 : 1] = bv;
+        }
+        return MAG_OK;
+    }
+
+    int autotune(int reps) {
+        if (mixed) {
+            MAG_TRY(tune_precision<float>(reps, st32, U32, F32, Uaux32));
+            if (p.n_stout > 0) {
+                // the FP64 forward smearing of the Hamiltonian
+                double best = 1e300;
+                for (int v = 0; v < kNumVariants; v++) {
+                    double ms = 0.0;
+                    StoutBufs<double> b = st64;
+                    MAG_TRY(time_one<double>(KF_STOUT_FWD, v, reps, b, U, F, Ubak, &ms));
+                    if (ms < best) {
+                        best = ms;
+                        tune[KF_STOUT_FWD][0] = v;
+                    }
+                }
+            }
+        } else {
+            MAG_TRY(tune_precision<double>(reps, st64, U, F, Uaux));
+        }
+        tuned = true;
+        return MAG_OK;
+    }
+    int ensure_tuned() { return tuned ? MAG_OK : autotune(3); }
 
     void hamiltonian_sums(bool is_new) {
         launch_kinetic_sum(geom, P, partial, sums, is_new ? SLOT_KIN_NEW : SLOT_KIN_OLD, stream);
@@ -374,6 +462,7 @@ struct mag_ctx {
 
     int build_graph() {
         if (graph) return MAG_OK;
+        MAG_TRY(ensure_tuned());
         cudaGraph_t g;
         MAG_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         int r = trajectory_body(true);
@@ -612,16 +701,17 @@ int mag_staple(mag_ctx* ctx, int chain, double* host) {
     if (ctx->mixed) {
         LinkPlanes<float> cur = ctx->U32;
         for (int k = 0; k < ctx->p.n_stout; k++) {
-            launch_stout_forward<float>(ctx->geom, cur, ctx->st32.lv[k], ctx->st32.Q[k], ctx->stream);
+            launch_stout_forward<float>(ctx->geom, cur, ctx->st32.lv[k], ctx->st32.Q[k],
+                                        ctx->var<float>(KF_STOUT_FWD), ctx->stream);
             cur = ctx->st32.lv[k];
         }
         LinkPlanes<float> z = ctx->p.n_stout ? ctx->st32.za : ctx->Uaux32;
-        launch_staple_dagger<float>(ctx->geom, cur, z, ctx->iwasaki, ctx->stream);
+        launch_staple_dagger<float>(ctx->geom, cur, z, ctx->iwasaki, ctx->var<float>(KF_STAPLE), ctx->stream);
         launch_links_to_aos_t<float>(z, ci.off, ci.V, ctx->staging, ctx->stream);
     } else {
         LinkPlanes<double> cur = ctx->smear64();
         LinkPlanes<double> z = ctx->p.n_stout ? ctx->st64.za : ctx->Uaux;
-        launch_staple_dagger<double>(ctx->geom, cur, z, ctx->iwasaki, ctx->stream);
+        launch_staple_dagger<double>(ctx->geom, cur, z, ctx->iwasaki, ctx->var<double>(KF_STAPLE), ctx->stream);
         launch_links_to_aos_t<double>(z, ci.off, ci.V, ctx->staging, ctx->stream);
     }
     MAG_TRY(ctx->check("mag_staple"));
@@ -739,12 +829,14 @@ int mag_stout_level(mag_ctx* ctx, int chain, int level, double* host) {
 
 int mag_integrate(mag_ctx* ctx) {
     if (!ctx) return MAG_ERR_ARG;
+    MAG_TRY(ctx->ensure_tuned());
     MAG_TRY(ctx->integrate());
     return ctx->sync("mag_integrate");
 }
 
 int mag_trajectory(mag_ctx* ctx, int refresh, mag_traj_result* results) {
     if (!ctx) return MAG_ERR_ARG;
+    MAG_TRY(ctx->ensure_tuned());
     MAG_TRY(ctx->trajectory_body(refresh != 0));
     std::vector<TrajRecord> r(ctx->nchain);
     MAG_CUDA(cudaMemcpyAsync(r.data(), ctx->rec, sizeof(TrajRecord) * ctx->nchain, cudaMemcpyDeviceToHost,
@@ -812,6 +904,12 @@ int mag_last_run_ms(mag_ctx* ctx, double* total_ms) {
     return MAG_OK;
 }
 
+int mag_last_measure_ms(mag_ctx* ctx, double* ms) {
+    if (!ctx || !ms) return MAG_ERR_ARG;
+    *ms = ctx->last_measure_ms;
+    return MAG_OK;
+}
+
 int mag_time_force(mag_ctx* ctx, int reps, double* ms) {
     if (!ctx || !ms || reps < 1) return MAG_ERR_ARG;
     auto once = [&]() {
@@ -833,69 +931,69 @@ int mag_time_force(mag_ctx* ctx, int reps, double* ms) {
 int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms) {
     if (!ctx || !which || !ms || reps < 1) return MAG_ERR_ARG;
     const std::string w(which);
-    std::function<void()> f;
     const bool m = ctx->mixed;
     const int L = ctx->p.n_stout;
     auto& g = ctx->geom;
     cudaStream_t s = ctx->stream;
-    if ((w == "stout_forward" || w == "stout_lambda" || w == "stout_chain") && L == 0)
-        return fail(MAG_ERR_STATE, "mag_time_kernel: no stout levels in this context");
+    static const char* fam_names[KF_COUNT] = {"force", "staple", "stout_forward", "stout_lambda", "stout_chain"};
+    int fam = -1;
+    for (int f = 0; f < KF_COUNT; f++)
+        if (w == fam_names[f]) fam = f;
+    if (fam >= KF_STOUT_FWD && L == 0) return fail(MAG_ERR_STATE, "mag_time_kernel: no stout levels in this context");
+    MAG_TRY(ctx->ensure_tuned());
     // one full force evaluation first, so every intermediate buffer holds live data
     if (m) ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
     else ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
-    if (w == "force") {
-        f = [&]() {
-            if (m) launch_force<float>(g, ctx->U32, ctx->F32, ctx->iwasaki, s);
-            else launch_force<double>(g, ctx->U, ctx->F, ctx->iwasaki, s);
-        };
-    } else if (w == "staple") {
-        f = [&]() {
-            if (m) launch_staple_dagger<float>(g, L ? ctx->st32.lv[L - 1] : ctx->U32, L ? ctx->st32.za : ctx->Uaux32,
-                                               ctx->iwasaki, s);
-            else launch_staple_dagger<double>(g, L ? ctx->st64.lv[L - 1] : ctx->U, L ? ctx->st64.za : ctx->Uaux,
-                                              ctx->iwasaki, s);
-        };
-    } else if (w == "stout_forward") {
-        f = [&]() {
-            if (m) launch_stout_forward<float>(g, ctx->U32, ctx->st32.lv[0], ctx->st32.Q[0], s);
-            else launch_stout_forward<double>(g, ctx->U, ctx->st64.lv[0], ctx->st64.Q[0], s);
-        };
-    } else if (w == "stout_lambda") {
-        f = [&]() {
-            if (m) launch_stout_lambda<float>(g, ctx->U32, ctx->st32.Q[0], ctx->st32.za, ctx->st32.lam, ctx->st32.zp, s);
-            else launch_stout_lambda<double>(g, ctx->U, ctx->st64.Q[0], ctx->st64.za, ctx->st64.lam, ctx->st64.zp, s);
-        };
-    } else if (w == "stout_chain") {
-        f = [&]() {
-            if (m) launch_stout_chain<float>(g, ctx->U32, ctx->st32.lam, ctx->st32.zp, ctx->st32.za, s);
-            else launch_stout_chain<double>(g, ctx->U, ctx->st64.lam, ctx->st64.zp, ctx->st64.za, s);
-        };
-    } else if (w == "evolve") {
-        f = [&]() {
+    if (fam >= 0) {
+        const KernelFamily f = (KernelFamily)fam;
+        if (m) return ctx->time_one<float>(f, ctx->var<float>(f), reps, ctx->st32, ctx->U32, ctx->F32, ctx->Uaux32, ms);
+        return ctx->time_one<double>(f, ctx->var<double>(f), reps, ctx->st64, ctx->U, ctx->F, ctx->Uaux, ms);
+    }
+    std::function<void()> fn;
+    if (w == "evolve") {
+        fn = [&]() {
             launch_evolve<double, double>(g, ctx->U, ctx->Ubak, ctx->P, 1e-3,
                                           m ? ctx->Uaux32 : LinkPlanes<float>{nullptr, 0}, s);
         };
     } else if (w == "kick") {
-        f = [&]() {
+        fn = [&]() {
             if (m) launch_kick<float>(g, ctx->P, ctx->F32, 0.0, s);
             else launch_kick<double>(g, ctx->P, ctx->F, 0.0, s);
         };
     } else if (w == "action") {
-        f = [&]() {
+        fn = [&]() {
             launch_action_sums<double>(g, ctx->U, true, ctx->partial, ctx->sums, SLOT_SCRATCH, SLOT_SCRATCH, s);
         };
     } else {
         return fail(MAG_ERR_ARG, "mag_time_kernel: unknown kernel '" + w + "'");
     }
-    f();
+    fn();
     MAG_TRY(ctx->sync("mag_time_kernel warm-up"));
     MAG_CUDA(cudaEventRecord(ctx->ev0, s));
-    for (int i = 0; i < reps; i++) f();
+    for (int i = 0; i < reps; i++) fn();
     MAG_CUDA(cudaEventRecord(ctx->ev1, s));
     MAG_TRY(ctx->sync("mag_time_kernel"));
     float t = 0.f;
     MAG_CUDA(cudaEventElapsedTime(&t, ctx->ev0, ctx->ev1));
     *ms = t / reps;
+    return MAG_OK;
+}
+
+int mag_autotune(mag_ctx* ctx, int reps, char* report, size_t len) {
+    if (!ctx || reps < 1) return MAG_ERR_ARG;
+    MAG_TRY(ctx->autotune(reps));
+    if (report && len) {
+        static const char* fam_names[KF_COUNT] = {"force", "staple", "stout_forward", "stout_lambda", "stout_chain"};
+        static const int minb[kNumVariants] = {2, 3, 4, 5};
+        std::string r = "{";
+        for (int f = 0; f < KF_COUNT; f++) {
+            if (f) r += ", ";
+            r += std::string("\"") + fam_names[f] + "\": [" + std::to_string(minb[ctx->tune[f][0]]) + ", " +
+                 std::to_string(minb[ctx->tune[f][1]]) + "]";
+        }
+        r += "}";
+        std::snprintf(report, len, "%s", r.c_str());
+    }
     return MAG_OK;
 }
 
@@ -907,7 +1005,7 @@ int mag_graph_kernel_count(mag_ctx* ctx, int* kernels) {
 }
 
 int mag_probe_fma_peak(int precision, double* tflops) {
-    if (!tflops || precision < 0 || precision > 1) return MAG_ERR_ARG;
+    if (!tflops || precision < 0 || precision > 2) return MAG_ERR_ARG;
     int dev = 0, sms = 0;
     MAG_CUDA(cudaGetDevice(&dev));
     MAG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -921,7 +1019,8 @@ int mag_probe_fma_peak(int precision, double* tflops) {
     for (int rep = 0; rep < 6; rep++) {
         cudaEventRecord(a, 0);
         if (precision == 0) launch_fma_probe<double>((double*)out, nblocks, iters, 0);
-        else launch_fma_probe<float>((float*)out, nblocks, iters, 0);
+        else if (precision == 1) launch_fma_probe<float>((float*)out, nblocks, iters, 0);
+        else launch_ffma2_probe(out, nblocks, iters, 0);
         cudaEventRecord(b, 0);
         cudaEventSynchronize(b);
         float ms = 0.f;
@@ -932,7 +1031,8 @@ int mag_probe_fma_peak(int precision, double* tflops) {
     cudaEventDestroy(b);
     cudaFree(out);
     MAG_CUDA(cudaGetLastError());
-    *tflops = 2.0 * 8.0 * iters * (double)nblocks * 256 / (best * 1e-3) / 1e12;
+    // two flops per FMA; a packed f32x2 FMA is two FMAs
+    *tflops = (precision == 2 ? 4.0 : 2.0) * 8.0 * iters * (double)nblocks * 256 / (best * 1e-3) / 1e12;
     return MAG_OK;
 }
 
@@ -991,12 +1091,17 @@ int mag_wilson_loops(mag_ctx* ctx, int chain, int Rmax, int Tmax, double* out) {
     LinkPlanes<double> lines{ctx->wl_lines, vp};
     LinkPlanes<double> tl{ctx->wl_lines + (size_t)Rmax * 9 * vp, vp};
     LinkPlanes<double> tl2{ctx->wl_lines + (size_t)(Rmax + 1) * 9 * vp, vp};
+    MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     launch_wilson_planar(ctx->geom, ctx->U, Rmax, Tmax, lines, tl, tl2, ctx->wl_partial, ctx->wl_out, ctx->stream);
+    MAG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
     MAG_TRY(ctx->check("mag_wilson_loops"));
     const size_t n = (size_t)3 * Tmax * ctx->nchain * Rmax;
     std::vector<dd2> h(n);
     MAG_CUDA(cudaMemcpyAsync(h.data(), ctx->wl_out, sizeof(dd2) * n, cudaMemcpyDeviceToHost, ctx->stream));
     MAG_TRY(ctx->sync("mag_wilson_loops"));
+    float wl_ms = 0.f;
+    MAG_CUDA(cudaEventElapsedTime(&wl_ms, ctx->ev0, ctx->ev1));
+    ctx->last_measure_ms = wl_ms;
     const double norm = 3.0 * ctx->hc[chain].V;  // perm.size() * V (field-wloop.h:98)
     for (int R = 1; R <= Rmax; R++)
         for (int T = 1; T <= Tmax; T++) {

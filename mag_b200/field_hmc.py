@@ -249,6 +249,11 @@ class Chmc:
         check(self._lib.mag_last_run_ms(self._h, ctypes.byref(v)), "mag_last_run_ms")
         return v.value
 
+    def last_measure_ms(self) -> float:
+        v = ctypes.c_double()
+        check(self._lib.mag_last_measure_ms(self._h, ctypes.byref(v)), "mag_last_measure_ms")
+        return v.value
+
     def time_force(self, reps: int) -> float:
         v = ctypes.c_double()
         check(self._lib.mag_time_force(self._h, int(reps), ctypes.byref(v)), "mag_time_force")
@@ -259,6 +264,14 @@ class Chmc:
         check(self._lib.mag_time_kernel(self._h, which.encode(), int(reps), ctypes.byref(v)), "mag_time_kernel")
         return v.value
 
+    def autotune(self, reps: int = 3) -> dict:
+        """Re-run the register-cap tuner; returns {family: [minB FP64, minB FP32]}."""
+        import json
+
+        buf = ctypes.create_string_buffer(1024)
+        check(self._lib.mag_autotune(self._h, int(reps), buf, len(buf)), "mag_autotune")
+        return json.loads(buf.value.decode())
+
     def graph_kernel_count(self) -> int:
         v = ctypes.c_int()
         check(self._lib.mag_graph_kernel_count(self._h, ctypes.byref(v)), "mag_graph_kernel_count")
@@ -268,5 +281,6 @@ class Chmc:
 def probe_fma_peak(precision: str = "fp64") -> float:
     """Measured CUDA-core FMA throughput of the current device (TFLOP/s, 2 flops per FMA)."""
     v = ctypes.c_double()
-    check(_lib.load().mag_probe_fma_peak(0 if precision == "fp64" else 1, ctypes.byref(v)), "mag_probe_fma_peak")
+    code = {"fp64": 0, "fp32": 1, "fp32x2": 2}[precision]
+    check(_lib.load().mag_probe_fma_peak(code, ctypes.byref(v)), "mag_probe_fma_peak")
     return v.value

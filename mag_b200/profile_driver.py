@@ -24,14 +24,22 @@ def main(argv=None) -> int:
     ap.add_argument("--mag", type=int, default=2)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--kernels", nargs="*", default=[])
+    ap.add_argument("--no-tune", action="store_true", help="keep the default variants (255-register cap)")
+    ap.add_argument("--probe", action="store_true", help="also report the FMA throughput probes")
     a = ap.parse_args(argv)
     with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1,
                 precision=a.precision, seed=1) as c:
         c.hot_start(1)
-        out = {"dims": a.dims, "precision": a.precision, "n_stout": a.n_stout,
-               "force_eval_ms": c.time_force(a.reps)}
+        out = {"dims": a.dims, "precision": a.precision, "n_stout": a.n_stout}
+        if not a.no_tune:
+            out["tuned_min_blocks"] = c.autotune(3)
+        out["force_eval_ms"] = c.time_force(a.reps)
         for k in a.kernels:
             out[f"{k}_ms"] = c.time_kernel(k, a.reps)
+    if a.probe:
+        from mag_b200.field_hmc import probe_fma_peak
+
+        out["fma_tflops"] = {p: probe_fma_peak(p) for p in ("fp64", "fp32", "fp32x2")}
     print(json.dumps(out))
     return 0
 
