@@ -4,8 +4,8 @@
 // float and double.  The staple and stout-derivative sums are reassociated so
 // that sub-products shared between paths are formed once: the values are the
 // reference sums (field-hmc.h:137-269, hep-lat/0311018 eq. 75 with
-// field-multi.h:180-269), the matmul count per link drops from 85 to 63
-// (Iwasaki staples) and from 66 to 37 (stout chain rule).
+// field-multi.h:180-269), the matmul count per link drops from 85 to 51
+// (Iwasaki staples, with double links) and from 66 to 37 (stout chain rule).
 #pragma once
 
 #include "lattice.cuh"
@@ -17,67 +17,63 @@ namespace magb {
 // paths are those of get_staple_dagger (field-hmc.h:226-239) and
 // get_rectangular_dagger (field-hmc.h:142-198).  The reference's
 // get_extended_staple_dagger returns A^dag.
+//
+// The 1x2 rectangles use the double links W_nu(y) = U_nu(y) U_nu(y+nu) of the
+// same field (k_double_link), so every path is two products:
+//   R1 = U_nu(x) W_mu(x+nu) U_nu^dag(x+2mu) . U_mu^dag(x+mu)
+//   R2 = U_nu^dag(x-nu) W_mu(x-nu) U_nu(x-nu+2mu) . U_mu^dag(x+mu)
+//   R5 = U_mu^dag(x-mu) . U_nu(x-mu) W_mu(x-mu+nu) U_nu^dag(x+mu)
+//   R6 = U_mu^dag(x-mu) . U_nu^dag(x-mu-nu) W_mu(x-mu-nu) U_nu(x-nu+mu)
+//   R3 = W_nu(x) U_mu(x+2nu) W_nu^dag(x+mu)
+//   R4 = W_nu^dag(x-2nu) U_mu(x-2nu) W_nu(x-2nu+mu)
+// with the common factors U_mu^dag(x+mu), U_mu^dag(x-mu) applied once to the
+// sums over nu.  Path products are special unitary: two rows are multiplied
+// and the third reconstructed.
 template <typename T, bool IWASAKI>
-MAG_HD mat3<T> staple_sum(const LinkPlanes<T>& U, const ChainInfo& ci, const Site& st, int mu) {
+MAG_HD mat3<T> staple_sum(const LinkPlanes<T>& U, const LinkPlanes<T>& W, const ChainInfo& ci, const Site& st,
+                          int mu) {
     mat3<T> A;
     set_zero(A);
     const T c0 = IWASAKI ? (T)ci.c0 : T(1);
     const T c1 = (T)ci.c1;
     if (IWASAKI) {
-        // R1 + R2 = [sum_nu U_nu(x)U_mu(x+nu)U_mu(x+mu+nu)U_nu^dag(x+2mu)
-        //          + U_nu^dag(x-nu)U_mu(x-nu)U_mu(x-nu+mu)U_nu(x-nu+2mu)] U_mu^dag(x+mu)
         mat3<T> acc;
         set_zero(acc);
 #pragma unroll 1
         for (int nu = 0; nu < 4; nu++) {
             if (nu == mu) continue;
-            mat3<T> t = mul(U.load(nu, st.g), U.load(mu, nb(ci, st, nu, 1)));
-            t = mul(t, U.load(mu, nb(ci, st, mu, 1, nu, 1)));
-            mul_nd_acc(acc, t, U.load(nu, nb(ci, st, mu, 2)));
-            t = mul_dn(U.load(nu, nb(ci, st, nu, -1)), U.load(mu, nb(ci, st, nu, -1)));
-            t = mul(t, U.load(mu, nb(ci, st, mu, 1, nu, -1)));
-            mul_acc(acc, t, U.load(nu, nb(ci, st, mu, 2, nu, -1)));
+            mat3<T> t = mul_2r(U.load_rows01(nu, st.g), W.load(mu, nb(ci, st, nu, 1)));
+            add_to(acc, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 2))));
+            t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), W.load(mu, nb(ci, st, nu, -1)));
+            add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 2, nu, -1))));
         }
         A = mul_nd(acc, U.load(mu, nb(ci, st, mu, 1)));
-        // R5 + R6 = U_mu^dag(x-mu) [sum_nu U_nu(x-mu)U_mu(x-mu+nu)U_mu(x+nu)U_nu^dag(x+mu)
-        //          + U_nu^dag(x-mu-nu)U_mu(x-mu-nu)U_mu(x-nu)U_nu(x-nu+mu)]
         set_zero(acc);
 #pragma unroll 1
         for (int nu = 0; nu < 4; nu++) {
             if (nu == mu) continue;
-            mat3<T> t = mul(U.load(nu, nb(ci, st, mu, -1)), U.load(mu, nb(ci, st, mu, -1, nu, 1)));
-            t = mul(t, U.load(mu, nb(ci, st, nu, 1)));
-            mul_nd_acc(acc, t, U.load(nu, nb(ci, st, mu, 1)));
-            t = mul_dn(U.load(nu, nb(ci, st, mu, -1, nu, -1)), U.load(mu, nb(ci, st, mu, -1, nu, -1)));
-            t = mul(t, U.load(mu, nb(ci, st, nu, -1)));
-            mul_acc(acc, t, U.load(nu, nb(ci, st, mu, 1, nu, -1)));
+            mat3<T> t = mul_2r(U.load_rows01(nu, nb(ci, st, mu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, 1)));
+            add_to(acc, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
+            t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, mu, -1, nu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, -1)));
+            add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
         }
         mul_dn_acc(A, U.load(mu, nb(ci, st, mu, -1)), acc);
         A = scaled(A, c1);
     }
-    // P_up + R3 = U_nu(x) [c0 U_mu(x+nu) + c1 U_nu(x+nu)U_mu(x+2nu)U_nu^dag(x+nu+mu)] U_nu^dag(x+mu)
-    // P_dn + R4 = U_nu^dag(x-nu) [c0 U_mu(x-nu) + c1 U_nu^dag(x-2nu)U_mu(x-2nu)U_nu(x-2nu+mu)] U_nu(x-nu+mu)
 #pragma unroll 1
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
-        mat3<T> Y = U.load(mu, nb(ci, st, nu, 1));
+        // P_up = U_nu(x) U_mu(x+nu) U_nu^dag(x+mu), P_dn = U_nu^dag(x-nu) U_mu(x-nu) U_nu(x-nu+mu)
+        mat3<T> t = mul_2r(U.load_rows01(nu, st.g), U.load(mu, nb(ci, st, nu, 1)));
+        axpy(A, c0, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
+        t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), U.load(mu, nb(ci, st, nu, -1)));
+        axpy(A, c0, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
         if (IWASAKI) {
-            Y = scaled(Y, c0);
-            const mat3<T> t = mul(U.load(nu, nb(ci, st, nu, 1)), U.load(mu, nb(ci, st, nu, 2)));
-            mat3<T> r = mul_nd(t, U.load(nu, nb(ci, st, mu, 1, nu, 1)));
-            axpy(Y, c1, r);
+            t = mul_2r(W.load_rows01(nu, st.g), U.load(mu, nb(ci, st, nu, 2)));
+            axpy(A, c1, mul_nd_su3(t, W.load(nu, nb(ci, st, mu, 1))));
+            t = mul_dn_2r(W.load_cols01(nu, nb(ci, st, nu, -2)), U.load(mu, nb(ci, st, nu, -2)));
+            axpy(A, c1, mul_su3(t, W.load(nu, nb(ci, st, mu, 1, nu, -2))));
         }
-        mat3<T> t = mul(U.load(nu, st.g), Y);
-        mul_nd_acc(A, t, U.load(nu, nb(ci, st, mu, 1)));
-        Y = U.load(mu, nb(ci, st, nu, -1));
-        if (IWASAKI) {
-            Y = scaled(Y, c0);
-            const mat3<T> t2 = mul_dn(U.load(nu, nb(ci, st, nu, -2)), U.load(mu, nb(ci, st, nu, -2)));
-            mat3<T> r = mul(t2, U.load(nu, nb(ci, st, mu, 1, nu, -2)));
-            axpy(Y, c1, r);
-        }
-        t = mul_dn(U.load(nu, nb(ci, st, nu, -1)), Y);
-        mul_acc(A, t, U.load(nu, nb(ci, st, mu, 1, nu, -1)));
     }
     return A;
 }
@@ -91,10 +87,10 @@ MAG_HD mat3<T> plaq_staple_sum(const LinkPlanes<T>& U, const ChainInfo& ci, cons
 #pragma unroll 1
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
-        mat3<T> t = mul(U.load(nu, st.g), U.load(mu, nb(ci, st, nu, 1)));
-        mul_nd_acc(A, t, U.load(nu, nb(ci, st, mu, 1)));
-        t = mul_dn(U.load(nu, nb(ci, st, nu, -1)), U.load(mu, nb(ci, st, nu, -1)));
-        mul_acc(A, t, U.load(nu, nb(ci, st, mu, 1, nu, -1)));
+        mat3<T> t = mul_2r(U.load_rows01(nu, st.g), U.load(mu, nb(ci, st, nu, 1)));
+        add_to(A, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
+        t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), U.load(mu, nb(ci, st, nu, -1)));
+        add_to(A, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
     }
     return A;
 }

@@ -63,10 +63,15 @@ struct AcceptArgs {
 constexpr int kNumVariants = 4;
 enum KernelFamily { KF_FORCE = 0, KF_STAPLE, KF_STOUT_FWD, KF_STOUT_LAMBDA, KF_STOUT_CHAIN, KF_COUNT };
 
+// W = double links U(x,mu) U(x+mu,mu); the Iwasaki staple kernels read W of the same field
 template <typename T>
-void launch_force(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, bool iwasaki, int v, cudaStream_t s);
+void launch_double_link(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, cudaStream_t s);
 template <typename T>
-void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> Z, bool iwasaki, int v, cudaStream_t s);
+void launch_force(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, AlgPlanes<T> F, bool iwasaki, int v,
+                  cudaStream_t s);
+template <typename T>
+void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, LinkPlanes<T> Z, bool iwasaki, int v,
+                          cudaStream_t s);
 template <typename T>
 void launch_constraint_fixup(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, cudaStream_t s);
 template <typename T>

@@ -31,26 +31,38 @@ __device__ __forceinline__ bool locate_link(const DevGeom& g, ChainInfo& ci, Sit
     return true;
 }
 
-// F(x,mu) = i beta/3 TA(U(x,mu) A^dag)   (field-hmc.h:394-421, free-link case)
-template <typename T, bool IWA, int MINB>
-__global__ void __launch_bounds__(kForceBlock, MINB) k_force(DevGeom g, LinkPlanes<T> U, AlgPlanes<T> F) {
+// W(x,mu) = U(x,mu) U(x+mu,mu): the double links of the 1x2 rectangles
+template <typename T>
+__global__ void __launch_bounds__(kForceBlock) k_double_link(DevGeom g, LinkPlanes<T> U, LinkPlanes<T> W) {
     ChainInfo ci;
     Site st;
     int mu;
     if (!locate_link(g, ci, st, mu)) return;
-    const mat3<T> A = staple_sum<T, IWA>(U, ci, st, mu);
+    W.store(mu, st.g, mul_su3(U.load(mu, st.g), U.load(mu, nb(ci, st, mu, 1))));
+}
+
+// F(x,mu) = i beta/3 TA(U(x,mu) A^dag)   (field-hmc.h:394-421, free-link case)
+template <typename T, bool IWA, int MINB>
+__global__ void __launch_bounds__(kForceBlock, MINB) k_force(DevGeom g, LinkPlanes<T> U, LinkPlanes<T> W,
+                                                           AlgPlanes<T> F) {
+    ChainInfo ci;
+    Site st;
+    int mu;
+    if (!locate_link(g, ci, st, mu)) return;
+    const mat3<T> A = staple_sum<T, IWA>(U, W, ci, st, mu);
     const mat3<T> M = mul_nd(U.load(mu, st.g), A);
     F.store(mu, st.g, i_times_ta(M, (T)(ci.beta / 3.0)));
 }
 
 // Z(x,mu) = A^dag  (get_extended_staple_dagger, field-hmc.h:262-269)
 template <typename T, bool IWA, int MINB>
-__global__ void __launch_bounds__(kForceBlock, MINB) k_staple_dagger(DevGeom g, LinkPlanes<T> U, LinkPlanes<T> Z) {
+__global__ void __launch_bounds__(kForceBlock, MINB) k_staple_dagger(DevGeom g, LinkPlanes<T> U, LinkPlanes<T> W,
+                                                                   LinkPlanes<T> Z) {
     ChainInfo ci;
     Site st;
     int mu;
     if (!locate_link(g, ci, st, mu)) return;
-    Z.store(mu, st.g, adj(staple_sum<T, IWA>(U, ci, st, mu)));
+    Z.store(mu, st.g, adj(staple_sum<T, IWA>(U, W, ci, st, mu)));
 }
 
 // Constrained segments (field-hmc.h:399-407): for a segment of `mag` links
@@ -160,18 +172,24 @@ unsigned link_blocks(const DevGeom& g) { return (unsigned)(4 * ((g.vpad + kForce
     }
 
 template <typename T>
-void launch_force(const DevGeom& g, LinkPlanes<T> U, AlgPlanes<T> F, bool iwasaki, int v, cudaStream_t s) {
-#define L_(M)                                                                         \
-    if (iwasaki) k_force<T, true, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, F); \
-    else k_force<T, false, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, F);
+void launch_double_link(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, cudaStream_t s) {
+    k_double_link<T><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, W);
+}
+template <typename T>
+void launch_force(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, AlgPlanes<T> F, bool iwasaki, int v,
+                  cudaStream_t s) {
+#define L_(M)                                                                            \
+    if (iwasaki) k_force<T, true, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, W, F); \
+    else k_force<T, false, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, W, F);
     MAG_BY_VARIANT(v, L_)
 #undef L_
 }
 template <typename T>
-void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> Z, bool iwasaki, int v, cudaStream_t s) {
-#define L_(M)                                                                                 \
-    if (iwasaki) k_staple_dagger<T, true, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, Z); \
-    else k_staple_dagger<T, false, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, Z);
+void launch_staple_dagger(const DevGeom& g, LinkPlanes<T> U, LinkPlanes<T> W, LinkPlanes<T> Z, bool iwasaki, int v,
+                          cudaStream_t s) {
+#define L_(M)                                                                                    \
+    if (iwasaki) k_staple_dagger<T, true, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, W, Z); \
+    else k_staple_dagger<T, false, M><<<link_blocks(g), kForceBlock, 0, s>>>(g, U, W, Z);
     MAG_BY_VARIANT(v, L_)
 #undef L_
 }
@@ -213,9 +231,11 @@ void launch_stout_chain_force(const DevGeom& g, LinkPlanes<T> Ul, AlgPlanes<T> L
 }
 
 #define MAG_INSTANTIATE(T)                                                                                      \
-    template void launch_force<T>(const DevGeom&, LinkPlanes<T>, AlgPlanes<T>, bool, int, cudaStream_t);       \
-    template void launch_staple_dagger<T>(const DevGeom&, LinkPlanes<T>, LinkPlanes<T>, bool, int,             \
-                                          cudaStream_t);                                                        \
+    template void launch_double_link<T>(const DevGeom&, LinkPlanes<T>, LinkPlanes<T>, cudaStream_t);           \
+    template void launch_force<T>(const DevGeom&, LinkPlanes<T>, LinkPlanes<T>, AlgPlanes<T>, bool, int,       \
+                                  cudaStream_t);                                                                \
+    template void launch_staple_dagger<T>(const DevGeom&, LinkPlanes<T>, LinkPlanes<T>, LinkPlanes<T>, bool,   \
+                                          int, cudaStream_t);                                                   \
     template void launch_constraint_fixup<T>(const DevGeom&, LinkPlanes<T>, AlgPlanes<T>, cudaStream_t);       \
     template void launch_stout_forward<T>(const DevGeom&, LinkPlanes<T>, LinkPlanes<T>, AlgPlanes<T>, int,     \
                                           cudaStream_t);                                                        \

@@ -6,10 +6,10 @@
 // one lookup, chunk2chain[g / MAG_CHUNK], maps a global site to its chain for
 // any block size that divides MAG_CHUNK.
 //
-// Plane layout (x0 fastest inside a chain, as qlat's index_from_coordinate):
-//   link field   : cplx<T> [4 mu][9 elements][Vpad]   (row-major 3x3)
-//   algebra field: T       [4 mu][8 compact  ][Vpad]   (see su3.cuh herm8)
-// A warp reads 32 consecutive sites of one plane: a 512-byte (double) or
+// Field layout (x0 fastest inside a chain, as qlat's index_from_coordinate):
+//   link field   : cplx<T> [4 mu][Vpad / 32 tiles][9 elements][32 sites]
+//   algebra field: T       [4 mu][Vpad / 32 tiles][8 compact ][32 sites]
+// A warp reads 32 consecutive sites of one element: a 512-byte (double) or
 // 256-byte (float) coalesced transaction per matrix element.
 #pragma once
 
@@ -78,21 +78,51 @@ MAG_HD int constraint_case(const ChainInfo& ci, const Site& st, int mu) {
     return 1;
 }
 
+// Inside one direction the sites are grouped in tiles of MAG_TILE consecutive
+// sites; a tile stores element 0 of its MAG_TILE links, then element 1, ...
+// (array-of-structure-of-arrays).  A warp of 32 consecutive sites still reads
+// one contiguous segment per element, and the elements of one link sit at
+// fixed offsets k * MAG_TILE from the first: one address per link, the rest
+// are immediate offsets.
+#define MAG_TILE 32
+
 template <typename T>
 struct LinkPlanes {
     cplx<T>* p;
     long vpad;
+    MAG_HD const cplx<T>* at(int mu, int g) const {
+        return p + (long)mu * 9 * vpad + (long)(g / MAG_TILE) * (9 * MAG_TILE) + (g % MAG_TILE);
+    }
     MAG_HD mat3<T> load(int mu, int g) const {
         mat3<T> m;
-        const cplx<T>* q = p + (long)mu * 9 * vpad + g;
+        const cplx<T>* q = at(mu, g);
 #pragma unroll
-        for (int k = 0; k < 9; k++) m.e[k / 3][k % 3] = q[(long)k * vpad];
+        for (int k = 0; k < 9; k++) m.e[k / 3][k % 3] = q[k * MAG_TILE];
+        return m;
+    }
+    // rows 0, 1 only (the left factor of a two-row product)
+    MAG_HD mat3<T> load_rows01(int mu, int g) const {
+        mat3<T> m;
+        const cplx<T>* q = at(mu, g);
+#pragma unroll
+        for (int k = 0; k < 6; k++) m.e[k / 3][k % 3] = q[k * MAG_TILE];
+        return m;
+    }
+    // columns 0, 1 only (the left factor U^dag of a two-row product)
+    MAG_HD mat3<T> load_cols01(int mu, int g) const {
+        mat3<T> m;
+        const cplx<T>* q = at(mu, g);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            m.e[r][0] = q[(3 * r) * MAG_TILE];
+            m.e[r][1] = q[(3 * r + 1) * MAG_TILE];
+        }
         return m;
     }
     MAG_HD void store(int mu, int g, const mat3<T>& m) const {
-        cplx<T>* q = p + (long)mu * 9 * vpad + g;
+        cplx<T>* q = const_cast<cplx<T>*>(at(mu, g));
 #pragma unroll
-        for (int k = 0; k < 9; k++) q[(long)k * vpad] = m.e[k / 3][k % 3];
+        for (int k = 0; k < 9; k++) q[k * MAG_TILE] = m.e[k / 3][k % 3];
     }
 };
 
@@ -100,17 +130,20 @@ template <typename T>
 struct AlgPlanes {
     T* p;
     long vpad;
+    MAG_HD const T* at(int mu, int g) const {
+        return p + (long)mu * 8 * vpad + (long)(g / MAG_TILE) * (8 * MAG_TILE) + (g % MAG_TILE);
+    }
     MAG_HD herm8<T> load(int mu, int g) const {
         herm8<T> q;
-        const T* b = p + (long)mu * 8 * vpad + g;
+        const T* b = at(mu, g);
 #pragma unroll
-        for (int k = 0; k < 8; k++) q.h[k] = b[(long)k * vpad];
+        for (int k = 0; k < 8; k++) q.h[k] = b[k * MAG_TILE];
         return q;
     }
     MAG_HD void store(int mu, int g, const herm8<T>& q) const {
-        T* b = p + (long)mu * 8 * vpad + g;
+        T* b = const_cast<T*>(at(mu, g));
 #pragma unroll
-        for (int k = 0; k < 8; k++) b[(long)k * vpad] = q.h[k];
+        for (int k = 0; k < 8; k++) b[k * MAG_TILE] = q.h[k];
     }
 };
 

@@ -241,10 +241,12 @@ struct mag_ctx {
             MAG_TRY(alloc_stout(st32, true));
             MAG_TRY(alloc_stout(st64, false));  // FP64 forward smearing for the Hamiltonian
             MAG_TRY(alloc_alg(F));              // FP64 force for single-call API use
+            if (iwasaki) MAG_TRY(alloc_links(W32));
         } else {
             MAG_TRY(alloc_links(Uaux));
             MAG_TRY(alloc_alg(F));
             MAG_TRY(alloc_stout(st64, true));
+            if (iwasaki) MAG_TRY(alloc_links(W64));
         }
         MAG_TRY(alloc((void**)&partial, sizeof(dd2) * 2 * (nchunk + 1)));
         MAG_TRY(alloc((void**)&sums, sizeof(dd2) * NUM_SLOTS * n));
@@ -280,17 +282,28 @@ struct mag_ctx {
         return tune[f][sizeof(T) == 8 ? 0 : 1];
     }
 
+    // double links of the field whose staples are being summed (Iwasaki only)
+    LinkPlanes<double> W64{nullptr, 0};
+    LinkPlanes<float> W32{nullptr, 0};
+    template <typename T>
+    LinkPlanes<T> wbuf() const {
+        if constexpr (sizeof(T) == 8) return W64;
+        else return W32;
+    }
+
     template <typename T>
     void force_eval(LinkPlanes<T> Uin, AlgPlanes<T> Fout, StoutBufs<T>& b) {
         if (p.n_stout == 0) {
-            launch_force<T>(geom, Uin, Fout, iwasaki, var<T>(KF_FORCE), stream);
+            if (iwasaki) launch_double_link<T>(geom, Uin, wbuf<T>(), stream);
+            launch_force<T>(geom, Uin, wbuf<T>(), Fout, iwasaki, var<T>(KF_FORCE), stream);
         } else {
             LinkPlanes<T> cur = Uin;
             for (int k = 0; k < p.n_stout; k++) {
                 launch_stout_forward<T>(geom, cur, b.lv[k], b.Q[k], var<T>(KF_STOUT_FWD), stream);
                 cur = b.lv[k];
             }
-            launch_staple_dagger<T>(geom, cur, b.za, iwasaki, var<T>(KF_STAPLE), stream);
+            if (iwasaki) launch_double_link<T>(geom, cur, wbuf<T>(), stream);
+            launch_staple_dagger<T>(geom, cur, wbuf<T>(), b.za, iwasaki, var<T>(KF_STAPLE), stream);
             for (int k = p.n_stout - 1; k >= 0; k--) {
                 LinkPlanes<T> ul = k == 0 ? Uin : b.lv[k - 1];
                 launch_stout_lambda<T>(geom, ul, b.Q[k], b.za, b.lam, b.zp, var<T>(KF_STOUT_LAMBDA), stream);
@@ -316,9 +329,9 @@ struct mag_ctx {
     void launch_one(KernelFamily f, int v, StoutBufs<T>& b, LinkPlanes<T> Uin, AlgPlanes<T> Fo, LinkPlanes<T> zs) {
         const int L = p.n_stout;
         switch (f) {
-            case KF_FORCE: launch_force<T>(geom, Uin, Fo, iwasaki, v, stream); break;
+            case KF_FORCE: launch_force<T>(geom, Uin, wbuf<T>(), Fo, iwasaki, v, stream); break;
             case KF_STAPLE:
-                launch_staple_dagger<T>(geom, L ? b.lv[L - 1] : Uin, L ? b.za : zs, iwasaki, v, stream);
+                launch_staple_dagger<T>(geom, L ? b.lv[L - 1] : Uin, wbuf<T>(), L ? b.za : zs, iwasaki, v, stream);
                 break;
             case KF_STOUT_FWD: launch_stout_forward<T>(geom, Uin, b.lv[0], b.Q[0], v, stream); break;
             case KF_STOUT_LAMBDA: launch_stout_lambda<T>(geom, Uin, b.Q[0], b.za, b.lam, b.zp, v, stream); break;
@@ -706,12 +719,16 @@ int mag_staple(mag_ctx* ctx, int chain, double* host) {
             cur = ctx->st32.lv[k];
         }
         LinkPlanes<float> z = ctx->p.n_stout ? ctx->st32.za : ctx->Uaux32;
-        launch_staple_dagger<float>(ctx->geom, cur, z, ctx->iwasaki, ctx->var<float>(KF_STAPLE), ctx->stream);
+        if (ctx->iwasaki) launch_double_link<float>(ctx->geom, cur, ctx->W32, ctx->stream);
+        launch_staple_dagger<float>(ctx->geom, cur, ctx->W32, z, ctx->iwasaki, ctx->var<float>(KF_STAPLE),
+                                    ctx->stream);
         launch_links_to_aos_t<float>(z, ci.off, ci.V, ctx->staging, ctx->stream);
     } else {
         LinkPlanes<double> cur = ctx->smear64();
         LinkPlanes<double> z = ctx->p.n_stout ? ctx->st64.za : ctx->Uaux;
-        launch_staple_dagger<double>(ctx->geom, cur, z, ctx->iwasaki, ctx->var<double>(KF_STAPLE), ctx->stream);
+        if (ctx->iwasaki) launch_double_link<double>(ctx->geom, cur, ctx->W64, ctx->stream);
+        launch_staple_dagger<double>(ctx->geom, cur, ctx->W64, z, ctx->iwasaki, ctx->var<double>(KF_STAPLE),
+                                     ctx->stream);
         launch_links_to_aos_t<double>(z, ci.off, ci.V, ctx->staging, ctx->stream);
     }
     MAG_TRY(ctx->check("mag_staple"));
