@@ -14,6 +14,8 @@
 #pragma once
 
 #include <stdint.h>
+#include <vector_functions.h>
+#include <vector_types.h>
 
 #include "su3.cuh"
 
@@ -88,6 +90,7 @@ MAG_HD int constraint_case(const ChainInfo& ci, const Site& st, int mu) {
 
 template <typename T>
 struct LinkPlanes {
+    static constexpr int kElems = 9;  // complex slots per link
     cplx<T>* p;
     long vpad;
     MAG_HD const cplx<T>* at(int mu, int g) const {
@@ -123,6 +126,66 @@ struct LinkPlanes {
         cplx<T>* q = const_cast<cplx<T>*>(at(mu, g));
 #pragma unroll
         for (int k = 0; k < 9; k++) q[k * MAG_TILE] = m.e[k / 3][k % 3];
+    }
+};
+
+// FP32 links: the nine complex elements travel in five 16-byte pairs
+// (0,1) (2,3) (4,5) (6,7) (8,-), so a link is five 128-bit loads instead of
+// nine 64-bit ones; same tile layout with pairs in place of elements.
+template <>
+struct LinkPlanes<float> {
+    static constexpr int kElems = 10;  // complex slots per link (one padding slot)
+    cplx<float>* p;
+    long vpad;
+    MAG_HD const float4* at(int mu, int g) const {
+        return reinterpret_cast<const float4*>(p) + (long)mu * 5 * vpad + (long)(g / MAG_TILE) * (5 * MAG_TILE) +
+               (g % MAG_TILE);
+    }
+    MAG_HD static void put(mat3<float>& m, int k, float re, float im) { m.e[k / 3][k % 3] = mk(re, im); }
+    MAG_HD mat3<float> load(int mu, int g) const {
+        mat3<float> m;
+        const float4* q = at(mu, g);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const float4 v = q[j * MAG_TILE];
+            put(m, 2 * j, v.x, v.y);
+            put(m, 2 * j + 1, v.z, v.w);
+        }
+        const float4 v = q[4 * MAG_TILE];
+        put(m, 8, v.x, v.y);
+        return m;
+    }
+    MAG_HD mat3<float> load_rows01(int mu, int g) const {
+        mat3<float> m;
+        const float4* q = at(mu, g);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const float4 v = q[j * MAG_TILE];
+            put(m, 2 * j, v.x, v.y);
+            put(m, 2 * j + 1, v.z, v.w);
+        }
+        return m;
+    }
+    MAG_HD mat3<float> load_cols01(int mu, int g) const {
+        mat3<float> m;
+        const float4* q = at(mu, g);
+        const float4 a = q[0], b = q[MAG_TILE], c = q[2 * MAG_TILE], d = q[3 * MAG_TILE];
+        put(m, 0, a.x, a.y);
+        put(m, 1, a.z, a.w);
+        put(m, 3, b.z, b.w);
+        put(m, 4, c.x, c.y);
+        put(m, 6, d.x, d.y);
+        put(m, 7, d.z, d.w);
+        return m;
+    }
+    MAG_HD void store(int mu, int g, const mat3<float>& m) const {
+        float4* q = const_cast<float4*>(at(mu, g));
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const cplx<float> a = m.e[(2 * j) / 3][(2 * j) % 3], b = m.e[(2 * j + 1) / 3][(2 * j + 1) % 3];
+            q[j * MAG_TILE] = make_float4(a.re, a.im, b.re, b.im);
+        }
+        q[4 * MAG_TILE] = make_float4(m.e[2][2].re, m.e[2][2].im, 0.f, 0.f);
     }
 };
 

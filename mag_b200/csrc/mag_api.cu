@@ -147,7 +147,7 @@ struct mag_ctx {
     template <typename T>
     int alloc_links(LinkPlanes<T>& l) {
         l.vpad = vpad;
-        return alloc((void**)&l.p, sizeof(cplx<T>) * 36 * (size_t)vpad);
+        return alloc((void**)&l.p, sizeof(cplx<T>) * 4 * LinkPlanes<T>::kElems * (size_t)vpad);
     }
     template <typename T>
     int alloc_alg(AlgPlanes<T>& a) {
