@@ -155,9 +155,28 @@ template <typename T>
 MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul, herm8<T>& lam, mat3<T>& zp) {
     const mat3<T> Q = expand(q);
     const mat3<T> QQ = mul(Q, Q);
-    double c0, c1;
-    ch_invariants(Q, QQ, c0, c1);
-    const ch_coef c = ch_coefficients<true>(c0, c1);
+    ch_coef_f cf;
+    ch_coef c;
+    bool nontrivial;
+    if constexpr (sizeof(T) == 4) {
+        nontrivial = ch_for<T, true>(Q, QQ, cf);  // FP32: power series (see su3.cuh)
+    } else {
+        double c0, c1;
+        ch_invariants(Q, QQ, c0, c1);
+        c = ch_coefficients<true>(c0, c1);  // FP64: the reference's closed form
+        nontrivial = !c.trivial;
+    }
+    if (!nontrivial) {
+        // c1 = 0: exp(iQ) = 1 and Lambda = 0 (field-multi.h:190)
+        zp = Z;
+        lam = herm_zero<T>();
+        return;
+    }
+    if constexpr (sizeof(T) == 4) {
+        c.f0r = cf.f0r; c.f0i = cf.f0i; c.f1r = cf.f1r; c.f1i = cf.f1i; c.f2r = cf.f2r; c.f2i = cf.f2i;
+        c.b10r = cf.b10r; c.b10i = cf.b10i; c.b11r = cf.b11r; c.b11i = cf.b11i; c.b12r = cf.b12r; c.b12i = cf.b12i;
+        c.b20r = cf.b20r; c.b20i = cf.b20i; c.b21r = cf.b21r; c.b21i = cf.b21i; c.b22r = cf.b22r; c.b22i = cf.b22i;
+    }
     const cplx<T> f0 = mk<T>((T)c.f0r, (T)c.f0i), f1 = mk<T>((T)c.f1r, (T)c.f1i), f2 = mk<T>((T)c.f2r, (T)c.f2i);
     // exp(iQ) and Z' exp(iQ)
     mat3<T> eq;
@@ -168,10 +187,6 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
 #pragma unroll
     for (int i = 0; i < 3; i++) eq.e[i][i] = eq.e[i][i] + f0;
     zp = mul(Z, eq);
-    if (c.trivial) {
-        lam = herm_zero<T>();
-        return;
-    }
     const mat3<T> W = mul(Ul, Z);  // U Sigma'
     const cplx<T> b10 = mk<T>((T)c.b10r, (T)c.b10i), b11 = mk<T>((T)c.b11r, (T)c.b11i),
                   b12 = mk<T>((T)c.b12r, (T)c.b12i);

@@ -571,6 +571,79 @@ MAG_HD ch_coef ch_coefficients(double c0, double c1) {
     return r;
 }
 
+// Single-precision Cayley-Hamilton coefficients by the power series of exp(iQ)
+// in the invariants.  For traceless Q, Q^3 = c1 Q + c0 with c0 = det Q =
+// Tr(Q^3)/3 and c1 = Tr(Q^2)/2, so Q^n = a_n + b_n Q + d_n Q^2 with
+//   a_{n+1} = c0 d_n,  b_{n+1} = a_n + c1 d_n,  d_{n+1} = b_n,
+// and f_j = sum_n i^n/n! (a_n, b_n, d_n)_j.  The derivative coefficients of
+// hep-lat/0311018 are b_1j = df_j/dc1 and b_2j = df_j/dc0 (dc1 = Tr(Q dQ),
+// dc0 = Tr(Q^2 dQ)), carried by differentiating the recurrence.  All terms
+// are real times a power of i, so nothing cancels beyond the alternating
+// series itself; with |eigenvalue| <= q = sqrt(4 c1 / 3) the sum stops when
+// q^n / n! < 1e-9.  Used by the FP32 kernels; returns false (and the caller
+// falls back to the double closed form) when q > 3.
+struct ch_coef_f {
+    float f0r, f0i, f1r, f1i, f2r, f2i;
+    float b10r, b10i, b11r, b11i, b12r, b12i;
+    float b20r, b20i, b21r, b21i, b22r, b22i;
+};
+
+template <bool WITH_B>
+MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
+    const float q2 = (4.f / 3.f) * c1;
+    if (q2 > 9.f) return false;
+    float a = 1.f, b = 0.f, d = 0.f;                       // Q^n coefficients
+    float a0 = 0.f, b0 = 0.f, d0 = 0.f, a1 = 0.f, b1 = 0.f, d1 = 0.f;  // d/dc0, d/dc1
+    float F[3][2] = {{1.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // f_j (re, im); n = 0 term
+    float B1[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    float B2[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    float coef = 1.f;    // 1/n!
+    float bound = 1.f;   // max(q, 1)^n / n!: the a_n, b_n, d_n and their derivatives
+                         // carry powers of q down to q^(n-5), so q < 1 counts as 1
+    const float q = fmaxf(sqrtf(q2), 1.f);
+#pragma unroll 1
+    for (int n = 1; n < 40; n++) {
+        // advance Q^{n-1} -> Q^n (and the derivatives)
+        const float na = c0 * d, nb = a + c1 * d, nd = b;
+        if (WITH_B) {
+            const float na0 = d + c0 * d0, nb0 = a0 + c1 * d0, nd0 = b0;
+            const float na1 = c0 * d1, nb1 = a1 + d + c1 * d1, nd1 = b1;
+            a0 = na0; b0 = nb0; d0 = nd0;
+            a1 = na1; b1 = nb1; d1 = nd1;
+        }
+        a = na; b = nb; d = nd;
+        coef /= (float)n;
+        bound *= q / (float)n;
+        // i^n/n!: real for even n (sign (-1)^{n/2}), imaginary for odd n
+        const int part = n & 1;
+        const float s = ((n >> 1) & 1) ? -coef : coef;
+        F[0][part] += s * a;
+        F[1][part] += s * b;
+        F[2][part] += s * d;
+        if (WITH_B) {
+            B1[0][part] += s * a1; B1[1][part] += s * b1; B1[2][part] += s * d1;
+            B2[0][part] += s * a0; B2[1][part] += s * b0; B2[2][part] += s * d0;
+        }
+        if (n > 5 && bound < 1e-9f) break;
+    }
+    r.f0r = F[0][0]; r.f0i = F[0][1]; r.f1r = F[1][0]; r.f1i = F[1][1]; r.f2r = F[2][0]; r.f2i = F[2][1];
+    r.b10r = B1[0][0]; r.b10i = B1[0][1]; r.b11r = B1[1][0]; r.b11i = B1[1][1]; r.b12r = B1[2][0]; r.b12i = B1[2][1];
+    r.b20r = B2[0][0]; r.b20i = B2[0][1]; r.b21r = B2[1][0]; r.b21i = B2[1][1]; r.b22r = B2[2][0]; r.b22i = B2[2][1];
+    return true;
+}
+
+// the same coefficients from the double closed form
+MAG_HD ch_coef_f ch_to_float(const ch_coef& c) {
+    ch_coef_f r;
+    r.f0r = (float)c.f0r; r.f0i = (float)c.f0i; r.f1r = (float)c.f1r; r.f1i = (float)c.f1i;
+    r.f2r = (float)c.f2r; r.f2i = (float)c.f2i;
+    r.b10r = (float)c.b10r; r.b10i = (float)c.b10i; r.b11r = (float)c.b11r; r.b11i = (float)c.b11i;
+    r.b12r = (float)c.b12r; r.b12i = (float)c.b12i;
+    r.b20r = (float)c.b20r; r.b20i = (float)c.b20i; r.b21r = (float)c.b21r; r.b21i = (float)c.b21i;
+    r.b22r = (float)c.b22r; r.b22i = (float)c.b22i;
+    return r;
+}
+
 // Q^2 of a compact Hermitian traceless matrix (Hermitian result)
 template <typename T>
 MAG_HD mat3<T> herm_square(const herm8<T>& q) {
@@ -593,23 +666,65 @@ MAG_HD void ch_invariants(const mat3<T>& Q, const mat3<T>& QQ, double& c0, doubl
     c1 = t2 / 2.0;
 }
 
+// single-precision invariants c0 = Re Tr(Q^3)/3, c1 = Re Tr(Q^2)/2
+MAG_HD void ch_invariants_f(const mat3<float>& Q, const mat3<float>& QQ, float& c0, float& c1) {
+    float t3 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) t3 += QQ.e[i][k].re * Q.e[k][i].re - QQ.e[i][k].im * Q.e[k][i].im;
+    c0 = t3 / 3.f;
+    c1 = 0.5f * (QQ.e[0][0].re + QQ.e[1][1].re + QQ.e[2][2].re);
+}
+
+// Cayley-Hamilton coefficients for a matrix of precision T: the reference's
+// closed form in double for T = double; the power series for T = float (the
+// closed form in double when the series would be too long).  trivial: c1 = 0,
+// where the reference returns exp(iQ) = 1 and Lambda = 0.
+template <typename T, bool WITH_B>
+MAG_HD bool ch_for(const mat3<T>& Q, const mat3<T>& QQ, ch_coef_f& cf) {
+    if constexpr (sizeof(T) == 4) {
+        float c0, c1;
+        ch_invariants_f(Q, QQ, c0, c1);
+        if (c1 == 0.f) return false;
+        if (ch_series<WITH_B>(c0, c1, cf)) return true;
+    }
+    double c0, c1;
+    ch_invariants(Q, QQ, c0, c1);
+    const ch_coef c = ch_coefficients<WITH_B>(c0, c1);
+    if (c.trivial) return false;
+    cf = ch_to_float(c);
+    return true;
+}
+
 // exp(iQ) = f0 + f1 Q + f2 Q^2 (field-hmc.h:82-123)
 template <typename T>
 MAG_HD mat3<T> expiQ(const herm8<T>& q) {
     const mat3<T> Q = expand(q);
     const mat3<T> QQ = mul(Q, Q);
-    double c0, c1;
-    ch_invariants(Q, QQ, c0, c1);
-    const ch_coef c = ch_coefficients<false>(c0, c1);
-    if (c.trivial) return unit_mat<T>();
+    cplx<T> f0, f1, f2;
+    if constexpr (sizeof(T) == 4) {
+        ch_coef_f c;
+        if (!ch_for<T, false>(Q, QQ, c)) return unit_mat<T>();
+        f0 = mk(c.f0r, c.f0i);
+        f1 = mk(c.f1r, c.f1i);
+        f2 = mk(c.f2r, c.f2i);
+    } else {
+        double c0, c1;
+        ch_invariants(Q, QQ, c0, c1);
+        const ch_coef c = ch_coefficients<false>(c0, c1);
+        if (c.trivial) return unit_mat<T>();
+        f0 = mk<T>((T)c.f0r, (T)c.f0i);
+        f1 = mk<T>((T)c.f1r, (T)c.f1i);
+        f2 = mk<T>((T)c.f2r, (T)c.f2i);
+    }
     mat3<T> r;
-    const cplx<T> f1 = mk<T>((T)c.f1r, (T)c.f1i), f2 = mk<T>((T)c.f2r, (T)c.f2i);
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) r.e[i][j] = f1 * Q.e[i][j] + f2 * QQ.e[i][j];
 #pragma unroll
-    for (int i = 0; i < 3; i++) r.e[i][i] = r.e[i][i] + mk<T>((T)c.f0r, (T)c.f0i);
+    for (int i = 0; i < 3; i++) r.e[i][i] = r.e[i][i] + f0;
     return r;
 }
 
