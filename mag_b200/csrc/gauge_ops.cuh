@@ -116,35 +116,35 @@ MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, cons
         // upper side: -i rho D [Lmu(x+nu) U_nu^dag(x) + U_nu^dag(x) Lnu(x)] + i rho Lnu(x+mu) E
         {
             const mat3<T> unx = U.load(nu, st.g);
-            const mat3<T> D = mul_nd(U.load(nu, nb(ci, st, mu, 1)), U.load(mu, nb(ci, st, nu, 1)));
-            const mat3<T> E = mul_nd(D, unx);
+            // D and E are products of links: two rows and a reconstructed third
+            const mat3<T> D = mul_nd_su3(U.load_rows01(nu, nb(ci, st, mu, 1)), U.load(mu, nb(ci, st, nu, 1)));
+            const mat3<T> E = mul_nd_su3(D, unx);
             add_to(sd, E);
-            mat3<T> inner = mul_nd(expand(Lam.load(mu, nb(ci, st, nu, 1))), unx);
-            mul_dn_acc(inner, unx, expand(Lam.load(nu, st.g)));
+            mat3<T> inner = mul_hm_nd(Lam.load(mu, nb(ci, st, nu, 1)), unx);
+            add_to(inner, mul_dn_mh(unx, Lam.load(nu, st.g)));
             mul_acc(ins, D, inner);
             // + i rho L E == -i rho (-L E)
-            const mat3<T> le = mul(expand(Lam.load(nu, nb(ci, st, mu, 1))), E);
-            sub_from(ins, le);
+            sub_from(ins, mul_hm(Lam.load(nu, nb(ci, st, mu, 1)), E));
         }
         // lower side: -i rho U_nu^dag(x-nu+mu) [U_mu^dag(x-nu)(Lmu(x-nu) - Lnu(x-nu)) U_nu(x-nu) + Lnu(x-nu+mu) G]
         {
             const int gm = nb(ci, st, nu, -1);
             const mat3<T> umn = U.load(mu, gm);
             const mat3<T> unn = U.load(nu, gm);
-            const mat3<T> G = mul_dn(umn, unn);
+            const mat3<T> G = mul_dn_su3(umn, unn);
             const mat3<T> undr = U.load(nu, nb(ci, st, mu, 1, nu, -1));
-            add_to(sd, mul_dn(undr, G));
+            add_to(sd, mul_dn_su3(undr, G));
             herm8<T> dl = Lam.load(mu, gm);
             const herm8<T> ln = Lam.load(nu, gm);
 #pragma unroll
             for (int k = 0; k < 8; k++) dl.h[k] -= ln.h[k];
-            mat3<T> inner = mul(mul_dn(umn, expand(dl)), unn);
-            mul_acc(inner, expand(Lam.load(nu, nb(ci, st, mu, 1, nu, -1))), G);
+            mat3<T> inner = mul(mul_dn_mh(umn, dl), unn);
+            add_to(inner, mul_hm(Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G));
             mul_dn_acc(ins, undr, inner);
         }
     }
     // acc += -i rho ins + i rho sd Lambda(x,mu)
-    mat3<T> own = mul(sd, expand(Lam.load(mu, st.g)));
+    mat3<T> own = mul_mh(sd, Lam.load(mu, st.g));
     sub_from(own, ins);
     add_to(acc, times_i(own, rho));
     return acc;
@@ -154,7 +154,7 @@ MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, cons
 template <typename T>
 MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul, herm8<T>& lam, mat3<T>& zp) {
     const mat3<T> Q = expand(q);
-    const mat3<T> QQ = mul(Q, Q);
+    const mat3<T> QQ = mul_hm(q, Q);
     ch_coef_f cf;
     ch_coef c;
     bool nontrivial;
@@ -198,8 +198,8 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
     const cplx<T> t1 = b10 * trW + b11 * trQW + b12 * trQQW;
     const cplx<T> t2 = b20 * trW + b21 * trQW + b22 * trQQW;
     // Gamma = t1 Q + t2 Q^2 + f1 W + f2 (Q W + W Q)
-    mat3<T> QW = mul(Q, W);
-    mul_acc(QW, W, Q);
+    mat3<T> QW = mul_hm(q, W);
+    add_to(QW, mul_mh(W, q));
     mat3<T> G;
 #pragma unroll
     for (int i = 0; i < 3; i++)

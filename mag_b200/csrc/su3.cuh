@@ -378,6 +378,97 @@ MAG_HD herm8<T> herm_zero() { herm8<T> q; for (int k = 0; k < 8; k++) q.h[k] = T
 template <typename T>
 MAG_HD herm8<T> scaled(const herm8<T>& a, T s) { herm8<T> q; for (int k = 0; k < 8; k++) q.h[k] = a.h[k] * s; return q; }
 
+// Products with a Hermitian traceless factor read straight from the compact
+// form: its diagonal is real, so an element costs one real-complex and two
+// complex-complex products.
+//   H = [[h0, z01, z02], [z01*, h1, z12], [z02*, z12*, -h0-h1]]
+template <typename T>
+MAG_HD void herm_rows(const herm8<T>& q, cplx<T> H[3][3]) {
+    H[0][0] = mk<T>(q.h[0], 0);
+    H[1][1] = mk<T>(q.h[1], 0);
+    H[2][2] = mk<T>(-q.h[0] - q.h[1], 0);
+    H[0][1] = mk<T>(q.h[2], q.h[3]);
+    H[1][0] = mk<T>(q.h[2], -q.h[3]);
+    H[0][2] = mk<T>(q.h[4], q.h[5]);
+    H[2][0] = mk<T>(q.h[4], -q.h[5]);
+    H[1][2] = mk<T>(q.h[6], q.h[7]);
+    H[2][1] = mk<T>(q.h[6], -q.h[7]);
+}
+template <typename T>
+MAG_HD cplx<T> rmul(T r, cplx<T> z) { return mk(r * z.re, r * z.im); }
+// H X
+template <typename T>
+MAG_HD mat3<T> mul_hm(const herm8<T>& q, const mat3<T>& x) {
+    cplx<T> H[3][3];
+    herm_rows(q, H);
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<T> s = rmul(H[i][i].re, x.e[i][j]);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                if (k != i) s = s + H[i][k] * x.e[k][j];
+            c.e[i][j] = s;
+        }
+    return c;
+}
+// H X^dag
+template <typename T>
+MAG_HD mat3<T> mul_hm_nd(const herm8<T>& q, const mat3<T>& x) {
+    cplx<T> H[3][3];
+    herm_rows(q, H);
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<T> s = rmul(H[i][i].re, conj(x.e[j][i]));
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                if (k != i) s = s + H[i][k] * conj(x.e[j][k]);
+            c.e[i][j] = s;
+        }
+    return c;
+}
+// X H
+template <typename T>
+MAG_HD mat3<T> mul_mh(const mat3<T>& x, const herm8<T>& q) {
+    cplx<T> H[3][3];
+    herm_rows(q, H);
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<T> s = rmul(H[j][j].re, x.e[i][j]);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                if (k != j) s = s + x.e[i][k] * H[k][j];
+            c.e[i][j] = s;
+        }
+    return c;
+}
+// X^dag H
+template <typename T>
+MAG_HD mat3<T> mul_dn_mh(const mat3<T>& x, const herm8<T>& q) {
+    cplx<T> H[3][3];
+    herm_rows(q, H);
+    mat3<T> c;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<T> s = rmul(H[j][j].re, conj(x.e[j][i]));
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+                if (k != j) s = s + conj(x.e[k][i]) * H[k][j];
+            c.e[i][j] = s;
+        }
+    return c;
+}
+
 // F = i s TA(M),  TA(M) = 1/2 (M - M^dag) - 1/6 Tr(M - M^dag)  (cps TrLessAntiHermMatrix)
 template <typename T>
 MAG_HD herm8<T> i_times_ta(const mat3<T>& m, T s) {
@@ -701,7 +792,7 @@ MAG_HD bool ch_for(const mat3<T>& Q, const mat3<T>& QQ, ch_coef_f& cf) {
 template <typename T>
 MAG_HD mat3<T> expiQ(const herm8<T>& q) {
     const mat3<T> Q = expand(q);
-    const mat3<T> QQ = mul(Q, Q);
+    const mat3<T> QQ = mul_hm(q, Q);
     cplx<T> f0, f1, f2;
     if constexpr (sizeof(T) == 4) {
         ch_coef_f c;
