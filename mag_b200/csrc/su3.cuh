@@ -17,8 +17,10 @@
 
 namespace magb {
 
+// Aligned to its size, so that one element is one 64-bit (float) or 128-bit
+// (double) memory access instead of two.
 template <typename T>
-struct cplx {
+struct alignas(2 * sizeof(T)) cplx {
     T re, im;
 };
 

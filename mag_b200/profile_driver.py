@@ -26,6 +26,8 @@ def main(argv=None) -> int:
     ap.add_argument("--kernels", nargs="*", default=[])
     ap.add_argument("--no-tune", action="store_true", help="keep the default variants (255-register cap)")
     ap.add_argument("--probe", action="store_true", help="also report the FMA throughput probes")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="wrap each --kernels timing loop in an NVTX range time_<kernel> (for ncu --nvtx-include)")
     a = ap.parse_args(argv)
     with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1,
                 precision=a.precision, seed=1) as c:
@@ -35,7 +37,13 @@ def main(argv=None) -> int:
             out["tuned_min_blocks"] = c.autotune(3)
         out["force_eval_ms"] = c.time_force(a.reps)
         for k in a.kernels:
+            if a.nvtx:
+                import torch
+
+                torch.cuda.nvtx.range_push(f"time_{k}")
             out[f"{k}_ms"] = c.time_kernel(k, a.reps)
+            if a.nvtx:
+                torch.cuda.nvtx.range_pop()
     if a.probe:
         from mag_b200.field_hmc import probe_fma_peak
 
