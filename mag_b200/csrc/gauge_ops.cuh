@@ -97,57 +97,55 @@ MAG_HD mat3<T> plaq_staple_sum(const LinkPlanes<T>& U, const ChainInfo& ci, cons
 
 // Chain rule of one stout level for link (x, mu), given Lambda on every link
 // and Zp = Z' exp(iQ) at (x, mu).  Returns
-//   Z = Z' e^{iQ} + i rho stp^dag Lambda(x,mu) + sum_nu [six insertion terms],
-// the insertion terms grouped around the shared products
+//   Z = Z' e^{iQ} + i rho [stp^dag Lambda(x,mu) - sum_nu (six insertion terms)],
+// the bracket T accumulated per staple, grouped around the shared products
 //   D = U_nu(x+mu) U_mu^dag(x+nu),  E = D U_nu^dag(x) = P_up^dag,
-//   G = U_mu^dag(x-nu) U_nu(x-nu),  U_nu^dag(x-nu+mu) G = P_dn^dag.
+//   G = U_mu^dag(x-nu) U_nu(x-nu),  U_nu^dag(x-nu+mu) G = P_dn^dag:
+//   upper: D [U_nu^dag(x) (L_mu(x) - L_nu(x)) - L_mu(x+nu) U_nu^dag(x)] + L_nu(x+mu) E
+//   lower: U_nu^dag(x-nu+mu) [G L_mu(x) - U_mu^dag(x-nu) (L_mu(x-nu) - L_nu(x-nu)) U_nu(x-nu)
+//                             - L_nu(x-nu+mu) G]
+// (stp^dag Lambda(x,mu) is distributed over the staples, so only T is live
+// across the loop).
 template <typename T>
-MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, const mat3<T>& Zp, const ChainInfo& ci,
-                           const Site& st, int mu) {
-    const T rho = (T)ci.rho;
-    mat3<T> acc = Zp;      // Z' e^{iQ}
-    mat3<T> sd;            // stp^dag
-    set_zero(sd);
-    mat3<T> ins;           // sum of insertion terms before the factor -i rho
-    set_zero(ins);
+MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, const LinkPlanes<T>& Zp,
+                           const ChainInfo& ci, const Site& st, int mu) {
+    const herm8<T> lx = Lam.load(mu, st.g);  // Lambda(x, mu)
+    mat3<T> t;
+    set_zero(t);
 #pragma unroll 1
     for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
-        // upper side: -i rho D [Lmu(x+nu) U_nu^dag(x) + U_nu^dag(x) Lnu(x)] + i rho Lnu(x+mu) E
         {
             const mat3<T> unx = U.load(nu, st.g);
             // D and E are products of links: two rows and a reconstructed third
             const mat3<T> D = mul_nd_su3(U.load_rows01(nu, nb(ci, st, mu, 1)), U.load(mu, nb(ci, st, nu, 1)));
             const mat3<T> E = mul_nd_su3(D, unx);
-            add_to(sd, E);
-            mat3<T> inner = mul_hm_nd(Lam.load(mu, nb(ci, st, nu, 1)), unx);
-            add_to(inner, mul_dn_mh(unx, Lam.load(nu, st.g)));
-            mul_acc(ins, D, inner);
-            // + i rho L E == -i rho (-L E)
-            sub_from(ins, mul_hm(Lam.load(nu, nb(ci, st, mu, 1)), E));
+            add_to(t, mul_hm(Lam.load(nu, nb(ci, st, mu, 1)), E));
+            herm8<T> dl = Lam.load(nu, st.g);
+#pragma unroll
+            for (int k = 0; k < 8; k++) dl.h[k] = lx.h[k] - dl.h[k];
+            mat3<T> inner = mul_dn_mh(unx, dl);
+            sub_from(inner, mul_hm_nd(Lam.load(mu, nb(ci, st, nu, 1)), unx));
+            mul_acc(t, D, inner);
         }
-        // lower side: -i rho U_nu^dag(x-nu+mu) [U_mu^dag(x-nu)(Lmu(x-nu) - Lnu(x-nu)) U_nu(x-nu) + Lnu(x-nu+mu) G]
         {
             const int gm = nb(ci, st, nu, -1);
             const mat3<T> umn = U.load(mu, gm);
             const mat3<T> unn = U.load(nu, gm);
             const mat3<T> G = mul_dn_su3(umn, unn);
-            const mat3<T> undr = U.load(nu, nb(ci, st, mu, 1, nu, -1));
-            add_to(sd, mul_dn_su3(undr, G));
             herm8<T> dl = Lam.load(mu, gm);
             const herm8<T> ln = Lam.load(nu, gm);
 #pragma unroll
             for (int k = 0; k < 8; k++) dl.h[k] -= ln.h[k];
-            mat3<T> inner = mul(mul_dn_mh(umn, dl), unn);
-            add_to(inner, mul_hm(Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G));
-            mul_dn_acc(ins, undr, inner);
+            mat3<T> inner = mul_mh(G, lx);
+            sub_from(inner, mul(mul_dn_mh(umn, dl), unn));
+            sub_from(inner, mul_hm(Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G));
+            mul_dn_acc(t, U.load(nu, nb(ci, st, mu, 1, nu, -1)), inner);
         }
     }
-    // acc += -i rho ins + i rho sd Lambda(x,mu)
-    mat3<T> own = mul_mh(sd, Lam.load(mu, st.g));
-    sub_from(own, ins);
-    add_to(acc, times_i(own, rho));
-    return acc;
+    mat3<T> z = Zp.load(mu, st.g);  // Z' e^{iQ}
+    add_to(z, times_i(t, (T)ci.rho));
+    return z;
 }
 
 // Lambda of compute_Lambda (field-multi.h:180-269) and Z' exp(iQ) for one link.

@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(kForceBlock, MINB) k_stout_chain(DevGeom g, Li
     Site st;
     int mu;
     if (!locate_link(g, ci, st, mu)) return;
-    const mat3<T> z = stout_chain(Ul, Lam, Zp.load(mu, st.g), ci, st, mu);
+    const mat3<T> z = stout_chain(Ul, Lam, Zp, ci, st, mu);
     if (TO_FORCE) {
         // thin level: F = i beta/3 TA(U Z)
         F.store(mu, st.g, i_times_ta(mul(Ul.load(mu, st.g), z), (T)(ci.beta / 3.0)));
