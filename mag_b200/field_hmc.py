@@ -100,6 +100,14 @@ class Chmc:
     def _field(self, chain: int) -> np.ndarray:
         return np.zeros((self.volume(chain), 4, 3, 3), np.complex128)
 
+    def _out_field(self, chain: int, out: np.ndarray | None) -> np.ndarray:
+        if out is None:
+            return self._field(chain)
+        shape = (self.volume(chain), 4, 3, 3)
+        if out.shape != shape or out.dtype != np.complex128 or not out.flags.c_contiguous or not out.flags.writeable:
+            raise ValueError(f"out must be a writeable C-contiguous complex128 array of shape {shape}")
+        return out
+
     def device_bytes(self) -> int:
         b = ctypes.c_size_t()
         check(self._lib.mag_ctx_device_bytes(self._h, ctypes.byref(b)), "mag_ctx_device_bytes")
@@ -111,8 +119,10 @@ class Chmc:
         assert U.shape == (self.volume(chain), 4, 3, 3)
         check(self._lib.mag_gauge_set(self._h, chain, _dp(U)), "mag_gauge_set")
 
-    def get_gauge(self, chain: int = 0) -> np.ndarray:
-        U = self._field(chain)
+    def get_gauge(self, chain: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        """The links of ``chain``; ``out`` (C-contiguous complex128, shape (V,4,3,3)),
+        e.g. a pinned buffer, receives them in place of a new array."""
+        U = self._out_field(chain, out)
         check(self._lib.mag_gauge_get(self._h, chain, _dp(U)), "mag_gauge_get")
         return U
 
@@ -130,8 +140,8 @@ class Chmc:
         P = np.ascontiguousarray(P, np.complex128)
         check(self._lib.mag_momentum_set(self._h, chain, _dp(P)), "mag_momentum_set")
 
-    def get_momentum(self, chain: int = 0) -> np.ndarray:
-        P = self._field(chain)
+    def get_momentum(self, chain: int = 0, out: np.ndarray | None = None) -> np.ndarray:
+        P = self._out_field(chain, out)
         check(self._lib.mag_momentum_get(self._h, chain, _dp(P)), "mag_momentum_get")
         return P
 
