@@ -36,6 +36,10 @@ extern "C" {
 #define MAG_ERR_NAN (-3)        /* NaN/Inf detected in a result */
 #define MAG_ERR_STATE (-4)      /* call not valid in the current state */
 #define MAG_ERR_NOMEM (-5)      /* device allocation failed */
+#define MAG_ERR_IO (-6)         /* file could not be opened, read or written */
+#define MAG_ERR_FORMAT (-7)     /* NERSC header: no END_HEADER, unknown DATATYPE, lattice size, short payload */
+#define MAG_ERR_CHECKSUM (-8)   /* NERSC CHECKSUM differs from the payload */
+#define MAG_ERR_PLAQUETTE (-9)  /* NERSC PLAQUETTE differs from the loaded links by more than 1e-4 */
 
 enum { MAG_ACTION_WILSON = 0, MAG_ACTION_IWASAKI = 1 };           /* qlat::Gauge::type */
 enum { MAG_PREC_FP64 = 0, MAG_PREC_MIXED = 1 };
@@ -151,6 +155,43 @@ int mag_wilson_loop(mag_ctx* ctx, int chain, const int r[3], int T, double* out)
 int mag_wilson_loops(mag_ctx* ctx, int chain, int Rmax, int Tmax, double* out);
 /* check_constrained_plaquette (field-matrix.h:407-443) */
 int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out);
+
+/* -------------------------------------------------------------- NERSC I/O */
+/* Header fields and payload digests of a NERSC configuration file.  The
+   payload is the lattice in site order x0 fastest, links mu = 0..3, each link
+   rows 0-1 (DATATYPE 4D_SU3_GAUGE, two_row = 1) or the full matrix
+   (4D_SU3_GAUGE_3x3), as big-endian IEEE-754 doubles. */
+typedef struct mag_nersc_info {
+    int dims[4];                /* DIMENSION_1..4 */
+    int two_row;                /* 1: 4D_SU3_GAUGE, 0: 4D_SU3_GAUGE_3x3 */
+    int64_t payload_offset;     /* bytes of the header (the payload follows END_HEADER) */
+    uint32_t checksum_header;   /* CHECKSUM (0 if absent) */
+    uint32_t checksum;          /* sum modulo 2^32 of the payload's 32-bit words in host byte order */
+    uint32_t crc32_header;      /* CRC32HASH (0 if absent) */
+    uint32_t crc32;             /* CRC-32 (zlib polynomial) of the host-order payload */
+    double plaquette_header;    /* PLAQUETTE (0 if absent) */
+    double plaquette;           /* avg_plaquette of the links */
+    double link_trace_header;   /* LINK_TRACE (0 if absent) */
+    double link_trace;          /* avg_real_trace of the links */
+} mag_nersc_info;
+
+/* import_config_nersc (field-matrix.h:594-713) into one chain: reads the
+   header (DATATYPE, DIMENSION_1..4, CHECKSUM, PLAQUETTE), checks the lattice
+   size, loads the payload, checks the word checksum (the links stay untouched
+   on a mismatch), rebuilds the third row of two-row files with reunitarize,
+   and checks the plaquette against the header to 1e-4 (the links are loaded
+   when this last check fails).  info (may be NULL) receives the header and the
+   computed digests.  Errors: MAG_ERR_IO, MAG_ERR_FORMAT, MAG_ERR_CHECKSUM,
+   MAG_ERR_PLAQUETTE (the reference asserts instead). */
+int mag_gauge_load_nersc(mag_ctx* ctx, int chain, const char* path, mag_nersc_info* info);
+/* export_config_nersc (field-matrix.h:452-572) of one chain with Arg_export
+   (beta, sequence_num, ensemble_label, field-matrix.h:445-450); two_row =
+   doesSkipThird.  CHECKSUM is the word sum of the host-order payload, the value
+   import_config_nersc checks; CRC32HASH the CRC-32 of the host-order payload. */
+int mag_gauge_save_nersc(mag_ctx* ctx, int chain, const char* path, int two_row, double beta,
+                         int sequence_number, const char* ensemble_label, mag_nersc_info* info);
+/* header only, no device work (computed fields are 0) */
+int mag_nersc_read_header(const char* path, mag_nersc_info* info);
 
 /* ------------------------------------------------------- allocation-free */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -36,6 +36,10 @@ int mag_graph_kernel_count(mag_ctx* ctx, int* kernels);
 /* measured CUDA-core FMA throughput of this device: precision 0 = FP64 FMA,
    1 = FP32 FMA, 2 = packed FP32 FMA (fma.rn.f32x2); tflops counts 2 flops per FMA */
 int mag_probe_fma_peak(int precision, double* tflops);
+/* CRC-32 (zlib) of n host bytes computed the way NERSC export/import does on
+   the device: seg-byte segment registers (seg a multiple of 16) chained with
+   the zero-byte shift; host only (tests the chaining without a GPU) */
+int mag_crc32_host(const void* data, size_t n, size_t seg, uint32_t* crc);
 
 #ifdef __cplusplus
 }

@@ -18,6 +18,10 @@ MAG_ERR_CUDA = -2
 MAG_ERR_NAN = -3
 MAG_ERR_STATE = -4
 MAG_ERR_NOMEM = -5
+MAG_ERR_IO = -6
+MAG_ERR_FORMAT = -7
+MAG_ERR_CHECKSUM = -8
+MAG_ERR_PLAQUETTE = -9
 
 ACTION_WILSON, ACTION_IWASAKI = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
@@ -59,6 +63,29 @@ class TrajResult(ctypes.Structure):
     def as_dict(self) -> dict:
         d = {n: getattr(self, n) for n, _ in self._fields_}
         d["demon"] = [self.demon[0], self.demon[1]]
+        return d
+
+
+class NerscInfo(ctypes.Structure):
+    """mag_nersc_info: NERSC header fields and the digests computed from the payload."""
+
+    _fields_ = [
+        ("dims", ctypes.c_int * 4),
+        ("two_row", ctypes.c_int),
+        ("payload_offset", ctypes.c_int64),
+        ("checksum_header", ctypes.c_uint32),
+        ("checksum", ctypes.c_uint32),
+        ("crc32_header", ctypes.c_uint32),
+        ("crc32", ctypes.c_uint32),
+        ("plaquette_header", ctypes.c_double),
+        ("plaquette", ctypes.c_double),
+        ("link_trace_header", ctypes.c_double),
+        ("link_trace", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {n: getattr(self, n) for n, _ in self._fields_}
+        d["dims"] = list(self.dims)
         return d
 
 
@@ -114,6 +141,11 @@ SIGNATURES = {
     "mag_autotune": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t],
     "mag_action_sums_noalloc": [_IP, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "mag_probe_fma_peak": [ctypes.c_int, _DP],
+    "mag_gauge_load_nersc": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
+    "mag_gauge_save_nersc": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                             ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
+    "mag_nersc_read_header": [ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
+    "mag_crc32_host": [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint32)],
 }
 _RESTYPE = {"mag_last_error": ctypes.c_char_p}
 

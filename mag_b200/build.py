@@ -16,8 +16,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmag_b200.so")
-SOURCES = ["kernels_force.cu", "kernels_update.cu", "kernels_wloop.cu", "mag_api.cu", "noalloc.cu"]
-HEADERS = ["su3.cuh", "lattice.cuh", "gauge_ops.cuh", "rng.cuh", "kernels.h"]
+SOURCES = ["kernels_force.cu", "kernels_update.cu", "kernels_wloop.cu", "kernels_nersc.cu", "mag_api.cu", "noalloc.cu",
+           "nersc_host.cpp"]
+HEADERS = ["su3.cuh", "lattice.cuh", "gauge_ops.cuh", "rng.cuh", "kernels.h", "nersc_host.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
@@ -31,7 +32,7 @@ def _newer(target: str, deps) -> bool:
 
 
 def _compile(src: str, verbose_ptxas: bool) -> str:
-    obj = os.path.join(OBJ, src.replace(".cu", ".o"))
+    obj = os.path.join(OBJ, os.path.splitext(src)[0] + ".o")
     deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS] + [
         os.path.join(ROOT, "include", "mag_c.h"), os.path.join(ROOT, "include", "mag_diag.h")]
     if _newer(obj, deps):

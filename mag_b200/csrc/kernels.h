@@ -44,7 +44,7 @@ struct ChainState {
 enum SumSlot {
     SLOT_PLAQ_OLD = 0, SLOT_RECT_OLD, SLOT_KIN_OLD,
     SLOT_PLAQ_NEW, SLOT_RECT_NEW, SLOT_KIN_NEW,
-    SLOT_PLAQ_THIN, SLOT_RECT_THIN, SLOT_SCRATCH,
+    SLOT_PLAQ_THIN, SLOT_RECT_THIN, SLOT_SCRATCH, SLOT_SCRATCH2,
     NUM_SLOTS
 };
 
@@ -133,6 +133,23 @@ template <typename T>
 void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s);
 // packed FP32 (fma.rn.f32x2): out holds nblocks * 256 float2
 void launch_ffma2_probe(void* out, int nblocks, int iters, cudaStream_t s);
+
+// sums[c][slot] = sum over the chain's links of ReTr U (avg_real_trace, field-matrix.h:391-405, times 12 V)
+void launch_link_trace_sum(const DevGeom& g, LinkPlanes<double> U, dd2* partial, dd2* sums, int slot,
+                           cudaStream_t s);
+
+// ---- NERSC payload (kernels_nersc.cu); payload = one chain's links in file order,
+// bytes a multiple of 16, 16-byte aligned
+// in place: big-endian <-> host order; *sum += 32-bit word sum of the host-order payload
+void launch_swap64_sum32(void* payload, size_t bytes, bool to_host, unsigned int* sum, cudaStream_t s);
+// z[i] = CRC-32 register (zlib polynomial, zero start, no final complement) of bytes [i*seg, (i+1)*seg)
+// of the payload; seg a multiple of 16
+void launch_crc32_segments(const void* payload, size_t bytes, size_t seg, uint32_t* z, cudaStream_t s);
+// host-order payload <-> links of the chain at site offset off (two_row: 6 complex per link, third row
+// rebuilt by reunitarize; else 9)
+void launch_payload_to_links(const double* payload, int two_row, int off, int V, LinkPlanes<double> U,
+                             cudaStream_t s);
+void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s);
 
 // ---- measurements (kernels_wloop.cu)
 // planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;

@@ -1,0 +1,179 @@
+// kernels_nersc.cu -- device side of NERSC configuration I/O
+// (export_config_nersc / import_config_nersc, field-matrix.h:452-713).
+//
+// The payload of a NERSC file is the lattice in lexicographic site order
+// (x0 fastest), four links per site, each link its first two rows
+// (DATATYPE 4D_SU3_GAUGE, 6 complex) or all three (4D_SU3_GAUGE_3x3,
+// 9 complex), every real an IEEE-754 binary64 in big-endian byte order.
+// The whole payload is staged in device memory and these kernels work on it
+// in place: byte order, the 32-bit word checksum, segment CRC-32 values, and
+// the conversion to and from the link tiles.  All are bound by HBM bandwidth.
+#include <stdint.h>
+
+#include "kernels.h"
+
+namespace magb {
+
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ uint64_t bswap64(uint64_t w) {
+    const uint32_t lo = (uint32_t)w, hi = (uint32_t)(w >> 32);
+    return ((uint64_t)__byte_perm(lo, 0, 0x0123) << 32) | (uint64_t)__byte_perm(hi, 0, 0x0123);
+}
+
+__device__ __forceinline__ uint32_t words32(uint64_t w) { return (uint32_t)w + (uint32_t)(w >> 32); }
+
+// sum of 32-bit words modulo 2^32 over the block, added to *sum (exact: the
+// sum is associative and commutative modulo 2^32, so the result is
+// independent of the launch shape)
+__device__ __forceinline__ void add_block_sum(uint32_t v, unsigned int* sum) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __shared__ uint32_t sm[kBlock / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) sm[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) atomicAdd(sum, v);
+    }
+}
+
+// n16 = payload bytes / 16.  to_host = 1: big-endian file words -> host order,
+// checksum of the host-order words; to_host = 0: checksum of the host-order
+// words, then -> big-endian.
+__global__ void k_swap64_sum32(ulonglong2* p, size_t n16, int to_host, unsigned int* sum) {
+    uint32_t s = 0;
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n16; i += stride) {
+        ulonglong2 v = p[i];
+        if (to_host) {
+            v.x = bswap64(v.x);
+            v.y = bswap64(v.y);
+            s += words32(v.x) + words32(v.y);
+        } else {
+            s += words32(v.x) + words32(v.y);
+            v.x = bswap64(v.x);
+            v.y = bswap64(v.y);
+        }
+        p[i] = v;
+    }
+    add_block_sum(s, sum);
+}
+
+// CRC-32 of the IEEE 802.3 / zlib polynomial (reflected 0xEDB88320), register
+// started at 0 and not complemented, of each `seg`-byte segment (the last one
+// may be shorter); the host chains the segment values with the linear
+// zero-byte shift.  Slicing by four: tab[k][b] is the register after byte b
+// followed by k zero bytes.
+__global__ void k_crc32_segments(const uint8_t* p, size_t n, size_t seg, uint32_t* z, size_t nseg) {
+    __shared__ uint32_t tab[4][256];
+    for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+        uint32_t c = (uint32_t)b;
+        for (int k = 0; k < 8; k++) c = (c >> 1) ^ (0xEDB88320u & (0u - (c & 1u)));
+        tab[0][b] = c;
+    }
+    __syncthreads();
+    for (int k = 1; k < 4; k++) {
+        for (int b = threadIdx.x; b < 256; b += blockDim.x) {
+            const uint32_t c = tab[k - 1][b];
+            tab[k][b] = (c >> 8) ^ tab[0][c & 0xffu];
+        }
+        __syncthreads();
+    }
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nseg) return;
+    const size_t b0 = i * seg;
+    const size_t b1 = b0 + seg < n ? b0 + seg : n;
+    uint32_t c = 0;
+    size_t b = b0;
+    // segments start on multiples of 16 bytes (seg is a multiple of 16)
+    const uint4* q = reinterpret_cast<const uint4*>(p + b0);
+    for (; b + 16 <= b1; b += 16, q++) {
+        const uint4 v = *q;
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            c ^= w[k];
+            c = tab[3][c & 0xffu] ^ tab[2][(c >> 8) & 0xffu] ^ tab[1][(c >> 16) & 0xffu] ^ tab[0][c >> 24];
+        }
+    }
+    for (; b < b1; b++) c = (c >> 8) ^ tab[0][(c ^ p[b]) & 0xffu];
+    z[i] = c;
+}
+
+// payload (host order) -> link tiles of one chain; NC = 6 rebuilds the third
+// row with the reference's reunitarize (field-matrix.h:83-100: CPS Unitarize
+// of rows 0, 1 unless both are zero), as import_config_nersc does after
+// copying the truncated matrices (field-matrix.h:680-690)
+template <int NC>
+__global__ void k_payload_to_links(const double* pay, int off, int V, LinkPlanes<double> U) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= V) return;
+    const int mu = blockIdx.y;
+    const double2* a = reinterpret_cast<const double2*>(pay) + ((size_t)s * 4 + mu) * NC;
+    mat3<double> m;
+    set_zero(m);
+#pragma unroll
+    for (int k = 0; k < NC; k++) {
+        const double2 v = a[k];
+        m.e[k / 3][k % 3] = mk(v.x, v.y);
+    }
+    if (NC == 6) {
+        bool all_zero = true;
+#pragma unroll
+        for (int k = 0; k < 6; k++) all_zero = all_zero && m.e[k / 3][k % 3].re == 0.0 && m.e[k / 3][k % 3].im == 0.0;
+        if (!all_zero) unitarize(m);
+    }
+    U.store(mu, off + s, m);
+}
+
+template <int NC>
+__global__ void k_links_to_payload(LinkPlanes<double> U, int off, int V, double* pay) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= V) return;
+    const int mu = blockIdx.y;
+    const mat3<double> m = U.load(mu, off + s);
+    double2* a = reinterpret_cast<double2*>(pay) + ((size_t)s * 4 + mu) * NC;
+#pragma unroll
+    for (int k = 0; k < NC; k++) a[k] = make_double2(m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im);
+}
+
+unsigned grid_for(size_t n, unsigned cap) {
+    const size_t b = (n + kBlock - 1) / kBlock;
+    return (unsigned)(b < cap ? (b ? b : 1) : cap);
+}
+
+}  // namespace
+
+void launch_swap64_sum32(void* payload, size_t bytes, bool to_host, unsigned int* sum, cudaStream_t s) {
+    const size_t n16 = bytes / 16;
+    // 148 SMs x 8 resident blocks of 256 threads: a grid-stride loop over the payload
+    k_swap64_sum32<<<grid_for(n16, 148 * 8), kBlock, 0, s>>>(static_cast<ulonglong2*>(payload), n16,
+                                                              to_host ? 1 : 0, sum);
+}
+
+void launch_crc32_segments(const void* payload, size_t bytes, size_t seg, uint32_t* z, cudaStream_t s) {
+    const size_t nseg = (bytes + seg - 1) / seg;
+    k_crc32_segments<<<grid_for(nseg, 1u << 30), kBlock, 0, s>>>(static_cast<const uint8_t*>(payload), bytes, seg,
+                                                                 z, nseg);
+}
+
+void launch_payload_to_links(const double* payload, int two_row, int off, int V, LinkPlanes<double> U,
+                             cudaStream_t s) {
+    const dim3 grid((V + kBlock - 1) / kBlock, 4);
+    if (two_row) k_payload_to_links<6><<<grid, kBlock, 0, s>>>(payload, off, V, U);
+    else k_payload_to_links<9><<<grid, kBlock, 0, s>>>(payload, off, V, U);
+}
+
+void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s) {
+    const dim3 grid((V + kBlock - 1) / kBlock, 4);
+    if (two_row) k_links_to_payload<6><<<grid, kBlock, 0, s>>>(U, off, V, payload);
+    else k_links_to_payload<9><<<grid, kBlock, 0, s>>>(U, off, V, payload);
+}
+
+}  // namespace magb

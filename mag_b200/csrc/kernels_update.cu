@@ -213,6 +213,20 @@ __global__ void k_kinetic_partials(DevGeom g, AlgPlanes<double> P, dd2* partial)
 }
 
 // per chain: sum the partials of its blocks in block order
+// sum over mu of ReTr U(x, mu) (avg_real_trace, field-matrix.h:391-405)
+__global__ void k_link_trace_partials(DevGeom g, LinkPlanes<double> U, dd2* partial) {
+    ChainInfo ci;
+    Site st;
+    dd2 k = {0.0, 0.0};
+    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st)) {
+        double acc = 0.0;
+#pragma unroll
+        for (int mu = 0; mu < 4; mu++) acc += retr(U.load(mu, st.g));
+        k.hi = acc;
+    }
+    k = block_reduce(k);
+    if (threadIdx.x == 0) partial[2 * blockIdx.x] = k;
+}
 __global__ void k_finalize(DevGeom g, const dd2* partial, int nq, dd2* sums, int slot0, double scale0) {
     const int c = blockIdx.x;
     const ChainInfo ci = g.chains[c];
@@ -496,6 +510,11 @@ template void launch_action_sums<double>(const DevGeom&, LinkPlanes<double>, boo
 template void launch_action_sums<float>(const DevGeom&, LinkPlanes<float>, bool, dd2*, dd2*, int, int,
                                         cudaStream_t);
 
+void launch_link_trace_sum(const DevGeom& g, LinkPlanes<double> U, dd2* partial, dd2* sums, int slot,
+                           cudaStream_t s) {
+    k_link_trace_partials<<<blocks(g), kBlock, 0, s>>>(g, U, partial);
+    k_finalize<<<g.nchain, kBlock, 0, s>>>(g, partial, 1, sums, slot, 1.0);
+}
 void launch_kinetic_sum(const DevGeom& g, AlgPlanes<double> P, dd2* partial, dd2* sums, int slot, cudaStream_t s) {
     k_kinetic_partials<<<blocks(g), kBlock, 0, s>>>(g, P, partial);
     k_finalize<<<g.nchain, kBlock, 0, s>>>(g, partial, 1, sums, slot, 0.5);

@@ -18,6 +18,7 @@
 #include "../../include/mag_c.h"
 #include "../../include/mag_diag.h"
 #include "kernels.h"
+#include "nersc_host.h"
 
 using namespace magb;
 
@@ -113,6 +114,10 @@ struct mag_ctx {
     bool uniform_override = false;
     double* staging = nullptr;
     long max_v = 0;
+    // NERSC I/O: pinned double buffer, CRC segment registers, word checksum
+    nersc::Pinned pin;
+    uint32_t* d_crc = nullptr;
+    unsigned int* d_csum = nullptr;
     long long host_traj = 0;
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0;
@@ -123,6 +128,7 @@ struct mag_ctx {
     ~mag_ctx() { release(); }
 
     void release() {
+        pin.release();
         if (graph) cudaGraphExecDestroy(graph);
         graph = nullptr;
         for (void* a : allocs) cudaFree(a);
@@ -1153,6 +1159,196 @@ int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out) {
     long coarse = 1;
     for (int d = 0; d < 4; d++) coarse *= ctx->hc[chain].L[d] / m;
     *out = s / (3.0 * (double)(coarse * npath));
+    return MAG_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------- NERSC I/O
+namespace {
+
+constexpr size_t kCrcSeg = 16384;          // bytes per CRC segment register
+constexpr size_t kIoChunk = 64u << 20;     // pinned chunk of the file <-> device copies
+
+void fill_info(mag_nersc_info* info, const nersc::Header& h, int two_row) {
+    memset(info, 0, sizeof(*info));
+    for (int d = 0; d < 4; d++) info->dims[d] = h.dims[d];
+    info->two_row = two_row;
+    info->payload_offset = h.payload_offset;
+    info->checksum_header = h.checksum;
+    info->crc32_header = h.crc32;
+    info->plaquette_header = h.plaquette;
+    info->link_trace_header = h.link_trace;
+}
+
+struct FileCloser {
+    FILE* f;
+    ~FileCloser() {
+        if (f) fclose(f);
+    }
+};
+
+int nersc_buffers(mag_ctx* ctx) {
+    std::string err;
+    int r = ctx->pin.ensure(kIoChunk, err);
+    if (r != MAG_OK) return fail(r, err);
+    if (!ctx->d_crc) {
+        const size_t nseg = (sizeof(double) * 72 * (size_t)ctx->max_v + kCrcSeg - 1) / kCrcSeg;
+        MAG_TRY(ctx->alloc((void**)&ctx->d_crc, sizeof(uint32_t) * nseg));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_csum, sizeof(unsigned int)));
+    }
+    return MAG_OK;
+}
+
+// avg_plaquette (field-matrix.h:387-389) and avg_real_trace (:391-405) of one chain
+int plaq_and_trace(mag_ctx* ctx, int chain, double* plaq, double* trace) {
+    launch_action_sums<double>(ctx->geom, ctx->U, false, ctx->partial, ctx->sums, SLOT_SCRATCH, SLOT_SCRATCH,
+                               ctx->stream);
+    launch_link_trace_sum(ctx->geom, ctx->U, ctx->partial, ctx->sums, SLOT_SCRATCH2, ctx->stream);
+    MAG_TRY(ctx->check("NERSC plaquette"));
+    std::vector<dd2> s;
+    MAG_TRY(ctx->read_sums(s));
+    const double V = (double)ctx->hc[chain].V;
+    const dd2 pl = s[chain * NUM_SLOTS + SLOT_SCRATCH], tr = s[chain * NUM_SLOTS + SLOT_SCRATCH2];
+    *plaq = (pl.hi + pl.lo) / (18.0 * V);
+    *trace = (tr.hi + tr.lo) / (12.0 * V);
+    return MAG_OK;
+}
+
+// CRC-32 of the host-order payload in staging and its 32-bit word sum; to_be
+// leaves the payload big-endian (export), else it is converted to host order
+// first (import)
+int payload_digest(mag_ctx* ctx, size_t bytes, bool import, uint32_t* crc, uint32_t* csum) {
+    const size_t nseg = (bytes + kCrcSeg - 1) / kCrcSeg;
+    MAG_CUDA(cudaMemsetAsync(ctx->d_csum, 0, sizeof(unsigned int), ctx->stream));
+    if (import) launch_swap64_sum32(ctx->staging, bytes, true, ctx->d_csum, ctx->stream);
+    launch_crc32_segments(ctx->staging, bytes, kCrcSeg, ctx->d_crc, ctx->stream);
+    if (!import) launch_swap64_sum32(ctx->staging, bytes, false, ctx->d_csum, ctx->stream);
+    MAG_TRY(ctx->check("NERSC payload digest"));
+    std::vector<uint32_t> z(nseg);
+    unsigned int sum = 0;
+    MAG_CUDA(cudaMemcpyAsync(z.data(), ctx->d_crc, sizeof(uint32_t) * nseg, cudaMemcpyDeviceToHost, ctx->stream));
+    MAG_CUDA(cudaMemcpyAsync(&sum, ctx->d_csum, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    MAG_TRY(ctx->sync("NERSC payload digest"));
+    *crc = nersc::crc32_chain(z.data(), nseg, kCrcSeg, bytes);
+    *csum = sum;
+    return MAG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mag_nersc_read_header(const char* path, mag_nersc_info* info) {
+    if (!path || !info) return fail(MAG_ERR_ARG, "mag_nersc_read_header: null argument");
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(MAG_ERR_IO, std::string("cannot open ") + path);
+    nersc::Header h;
+    std::string err;
+    int two_row = 0;
+    int r = nersc::read_header(fc.f, h, err);
+    if (r == MAG_OK) r = nersc::datatype_rows(h.datatype, two_row, err);
+    if (r != MAG_OK) return fail(r, std::string("import_config_nersc: ") + err);
+    fill_info(info, h, two_row);
+    return MAG_OK;
+}
+
+int mag_gauge_load_nersc(mag_ctx* ctx, int chain, const char* path, mag_nersc_info* info) {
+    if (!ctx || !path) return fail(MAG_ERR_ARG, "mag_gauge_load_nersc: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    FileCloser fc{fopen(path, "rb")};
+    if (!fc.f) return fail(MAG_ERR_IO, std::string("cannot open ") + path);
+    nersc::Header h;
+    std::string err;
+    int two_row = 0;
+    int r = nersc::read_header(fc.f, h, err);
+    if (r == MAG_OK) r = nersc::datatype_rows(h.datatype, two_row, err);
+    if (r != MAG_OK) return fail(r, std::string("import_config_nersc: ") + err);
+    for (int d = 0; d < 4; d++)
+        if (h.dims[d] != ci.L[d])
+            return fail(MAG_ERR_FORMAT, "import_config_nersc: WRONG Lattice Size (file " + std::to_string(h.dims[0]) +
+                                            "x" + std::to_string(h.dims[1]) + "x" + std::to_string(h.dims[2]) + "x" +
+                                            std::to_string(h.dims[3]) + ")");
+    MAG_TRY(nersc_buffers(ctx));
+    const size_t bytes = (size_t)ci.V * 4 * (two_row ? 6 : 9) * 16;
+    if (fseeko(fc.f, (off_t)h.payload_offset, SEEK_SET) != 0)
+        return fail(MAG_ERR_IO, "import_config_nersc: cannot seek to the payload");
+    r = nersc::file_to_device(fc.f, ctx->staging, bytes, ctx->pin, ctx->stream, err);
+    if (r != MAG_OK) return fail(r, "import_config_nersc: " + err);
+    uint32_t crc = 0, csum = 0;
+    MAG_TRY(payload_digest(ctx, bytes, true, &crc, &csum));
+    if (info) {
+        fill_info(info, h, two_row);
+        info->checksum = csum;
+        info->crc32 = crc;
+    }
+    // field-matrix.h:673-676 / :695-699: the links are left untouched on a checksum mismatch
+    if (csum != h.checksum) {
+        char b[128];
+        snprintf(b, sizeof(b), "import_config_nersc: WRONG Checksum: %x(labeled) vs %x(computed)", h.checksum, csum);
+        return fail(MAG_ERR_CHECKSUM, b);
+    }
+    launch_payload_to_links(ctx->staging, two_row, ci.off, ci.V, ctx->U, ctx->stream);
+    MAG_TRY(ctx->refresh_copy());
+    double plaq = 0.0, trace = 0.0;
+    MAG_TRY(plaq_and_trace(ctx, chain, &plaq, &trace));
+    if (info) {
+        info->plaquette = plaq;
+        info->link_trace = trace;
+    }
+    // field-matrix.h:708-711
+    if (std::fabs(plaq - h.plaquette) > 1e-4) {
+        char b[160];
+        snprintf(b, sizeof(b), "import_config_nersc: Plaquette: %.8f(labeled) vs %.8f(computed)", h.plaquette, plaq);
+        return fail(MAG_ERR_PLAQUETTE, b);
+    }
+    return MAG_OK;
+}
+
+int mag_gauge_save_nersc(mag_ctx* ctx, int chain, const char* path, int two_row, double beta,
+                         int sequence_number, const char* ensemble_label, mag_nersc_info* info) {
+    if (!ctx || !path) return fail(MAG_ERR_ARG, "mag_gauge_save_nersc: null argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    const ChainInfo& ci = ctx->hc[chain];
+    MAG_TRY(nersc_buffers(ctx));
+    double plaq = 0.0, trace = 0.0;
+    MAG_TRY(plaq_and_trace(ctx, chain, &plaq, &trace));
+    const size_t bytes = (size_t)ci.V * 4 * (two_row ? 6 : 9) * 16;
+    launch_links_to_payload(ctx->U, two_row ? 1 : 0, ci.off, ci.V, ctx->staging, ctx->stream);
+    uint32_t crc = 0, csum = 0;
+    MAG_TRY(payload_digest(ctx, bytes, false, &crc, &csum));
+    const std::string hdr = nersc::format_header(ci.L, two_row ? 1 : 0, crc, csum, trace, plaq, ensemble_label,
+                                                 sequence_number, beta, (long long)time(nullptr));
+    FileCloser fc{fopen(path, "wb")};
+    if (!fc.f) return fail(MAG_ERR_IO, std::string("cannot create ") + path);
+    if (fputs(hdr.c_str(), fc.f) < 0) return fail(MAG_ERR_IO, "export_config_nersc: header write failed");
+    std::string err;
+    const int r = nersc::device_to_file(ctx->staging, bytes, fc.f, ctx->pin, ctx->stream, err);
+    if (r != MAG_OK) return fail(r, "export_config_nersc: " + err);
+    const int cl = fclose(fc.f);
+    fc.f = nullptr;
+    if (cl != 0) return fail(MAG_ERR_IO, "export_config_nersc: close failed");
+    if (info) {
+        memset(info, 0, sizeof(*info));
+        for (int d = 0; d < 4; d++) info->dims[d] = ci.L[d];
+        info->two_row = two_row ? 1 : 0;
+        info->payload_offset = (int64_t)hdr.size();
+        info->checksum_header = info->checksum = csum;
+        info->crc32_header = info->crc32 = crc;
+        info->plaquette_header = info->plaquette = plaq;
+        info->link_trace_header = info->link_trace = trace;
+    }
+    return MAG_OK;
+}
+
+int mag_crc32_host(const void* data, size_t n, size_t seg, uint32_t* crc) {
+    if ((!data && n) || !crc || seg == 0 || seg % 16) return fail(MAG_ERR_ARG, "mag_crc32_host: bad argument");
+    const uint8_t* p = static_cast<const uint8_t*>(data);
+    const size_t nseg = (n + seg - 1) / seg;
+    std::vector<uint32_t> z(nseg);
+    for (size_t i = 0; i < nseg; i++) z[i] = nersc::crc32_register(p + i * seg, std::min(seg, n - i * seg));
+    *crc = nersc::crc32_chain(z.data(), nseg, seg, n);
     return MAG_OK;
 }
 

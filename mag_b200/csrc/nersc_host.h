@@ -1,0 +1,72 @@
+// nersc_host.h -- host side of NERSC configuration I/O (field-matrix.h:452-713):
+// header parsing and formatting, CRC-32 chaining, chunked file <-> device copies.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include <string>
+
+namespace magb {
+namespace nersc {
+
+// Fields of the header that import_config_nersc reads (field-matrix.h:605-650),
+// plus the optional ones export_config_nersc writes.
+struct Header {
+    std::string datatype;
+    int dims[4] = {0, 0, 0, 0};
+    bool has_checksum = false;
+    uint32_t checksum = 0;
+    bool has_plaquette = false;
+    double plaquette = 0.0;
+    bool has_link_trace = false;
+    double link_trace = 0.0;
+    bool has_crc32 = false;
+    uint32_t crc32 = 0;
+    long long payload_offset = -1;  // file offset just after the END_HEADER line
+};
+
+// Reads the header with the reference's rules: one line at a time; a line that
+// contains a keyword carries its value after the first '=' (blanks and tabs
+// skipped, one trailing newline removed); CHECKSUM is hexadecimal; the header
+// ends at the first line containing END_HEADER.  Returns MAG_OK, MAG_ERR_IO or
+// MAG_ERR_FORMAT (err holds the message).
+int read_header(FILE* f, Header& h, std::string& err);
+
+// DATATYPE -> rows stored per link: 4D_SU3_GAUGE -> two_row = 1,
+// 4D_SU3_GAUGE_3x3 -> 0; anything else is MAG_ERR_FORMAT.
+int datatype_rows(const std::string& datatype, int& two_row, std::string& err);
+
+// The header block export_config_nersc writes (field-matrix.h:486-508 and
+// :530-552), keys in the same order; LINK_TRACE, PLAQUETTE and BETA with 12
+// significant digits for the two-row type and 6 for 3x3 (the stream precision
+// of the reference).
+std::string format_header(const int dims[4], int two_row, uint32_t crc32, uint32_t checksum, double link_trace,
+                          double plaquette, const char* ensemble_label, int sequence_number, double beta,
+                          long long unix_time);
+
+// CRC-32 (zlib) of a byte string from per-segment registers: z[i] is the
+// register of segment i started at 0 (no complement), all segments `seg`
+// bytes except possibly the last; total = bytes of the string.
+uint32_t crc32_chain(const uint32_t* z, size_t nseg, size_t seg, size_t total);
+// register of one segment on the host (same definition as the device kernel)
+uint32_t crc32_register(const uint8_t* p, size_t n);
+
+// Pinned double buffer for chunked copies between a file and device memory.
+struct Pinned {
+    void* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    size_t chunk = 0;
+    int ensure(size_t chunk_bytes, std::string& err);
+    void release();
+};
+
+// read `bytes` from f (positioned at the payload) into device memory d
+// through the pinned buffers on `stream`; returns MAG_OK / MAG_ERR_IO / MAG_ERR_CUDA
+int file_to_device(FILE* f, void* d, size_t bytes, Pinned& pin, cudaStream_t stream, std::string& err);
+// write `bytes` of device memory d to f after the header
+int device_to_file(const void* d, size_t bytes, FILE* f, Pinned& pin, cudaStream_t stream, std::string& err);
+
+}  // namespace nersc
+}  // namespace magb

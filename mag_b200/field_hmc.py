@@ -253,6 +253,28 @@ class Chmc:
         check(self._lib.mag_constrained_plaquette(self._h, chain, ctypes.byref(v)), "mag_constrained_plaquette")
         return v.value
 
+    # ------------------------------------------------------------ NERSC I/O
+    def export_config_nersc(self, path: str, beta: float | None = None, sequence_num: int = 0,
+                            ensemble_label: str = "", skip_third: bool = True, chain: int = 0) -> dict:
+        """export_config_nersc (field-matrix.h:452-572) with Arg_export (beta,
+        sequence_num, ensemble_label); skip_third = doesSkipThird (DATATYPE
+        4D_SU3_GAUGE).  Returns the header fields written and the digests."""
+        info = _lib.NerscInfo()
+        b = self.params[chain].beta if beta is None else float(beta)
+        check(self._lib.mag_gauge_save_nersc(self._h, chain, str(path).encode(), 1 if skip_third else 0, b,
+                                             int(sequence_num), ensemble_label.encode(), ctypes.byref(info)),
+              "mag_gauge_save_nersc")
+        return info.as_dict()
+
+    def import_config_nersc(self, path: str, chain: int = 0) -> dict:
+        """import_config_nersc (field-matrix.h:594-713).  Raises MagError with
+        code MAG_ERR_FORMAT / MAG_ERR_CHECKSUM / MAG_ERR_PLAQUETTE / MAG_ERR_IO
+        where the reference asserts."""
+        info = _lib.NerscInfo()
+        check(self._lib.mag_gauge_load_nersc(self._h, chain, str(path).encode(), ctypes.byref(info)),
+              "mag_gauge_load_nersc")
+        return info.as_dict()
+
     # ------------------------------------------------------------ timing
     def last_run_ms(self) -> float:
         v = ctypes.c_double()
@@ -293,4 +315,19 @@ def probe_fma_peak(precision: str = "fp64") -> float:
     v = ctypes.c_double()
     code = {"fp64": 0, "fp32": 1, "fp32x2": 2}[precision]
     check(_lib.load().mag_probe_fma_peak(code, ctypes.byref(v)), "mag_probe_fma_peak")
+    return v.value
+
+
+def read_nersc_header(path: str) -> dict:
+    """The NERSC header fields of a file (no device work)."""
+    info = _lib.NerscInfo()
+    check(_lib.load().mag_nersc_read_header(str(path).encode(), ctypes.byref(info)), "mag_nersc_read_header")
+    return info.as_dict()
+
+
+def crc32_segmented(data: bytes, seg: int = 16384) -> int:
+    """CRC-32 of ``data`` by the segment-and-chain scheme of the NERSC kernels (host)."""
+    v = ctypes.c_uint32()
+    buf = ctypes.create_string_buffer(bytes(data), len(data))
+    check(_lib.load().mag_crc32_host(buf, len(data), int(seg), ctypes.byref(v)), "mag_crc32_host")
     return v.value
