@@ -58,6 +58,10 @@ WORKLOADS = {
     # 48^3 x 96, beta 2.37, 3 stout levels, 16 FG steps, mixed, Wilson loops R, T <= 8 after each trajectory
     "48x48x48x96_iwasaki_3stout_wloops": dict(dims=(48, 48, 48, 96), beta=2.37, n_stout=3, n_steps=16,
                                              precision="mixed", wilson=8),
+    # NERSC configuration load (import_config_nersc) of a 32^4 4D_SU3_GAUGE_3x3 file (604 MB payload);
+    # a step is one load from the page cache; the save (export_config_nersc) is timed beside it
+    "nersc_io_32x32x32x32": dict(dims=(32, 32, 32, 32), beta=2.25, n_stout=0, n_steps=1, precision="fp64",
+                                 kind="nersc"),
 }
 DEFAULT = "16x16x16x32_iwasaki_3stout"
 COMMON = dict(mag=2, action="iwasaki", c1=-0.331, rho=0.1, tau=1.0, accept="metropolis", integrator="fg")
@@ -460,6 +464,172 @@ def run_gpu(args, params, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- NERSC I/O workload
+NERSC_METRIC = "NERSC configuration load throughput (payload GB/s, import_config_nersc)"
+
+
+def nersc_dir(need_bytes: int) -> str:
+    """A scratch directory for the configuration files: /dev/shm when it has room, else the temp dir."""
+    import shutil
+    import tempfile
+
+    for base in ("/dev/shm", None):
+        try:
+            d = tempfile.mkdtemp(prefix="mag_nersc_", dir=base)
+        except OSError:
+            continue
+        if shutil.disk_usage(d).free > need_bytes + (1 << 30):
+            return d
+        shutil.rmtree(d, ignore_errors=True)
+    return tempfile.mkdtemp(prefix="mag_nersc_")
+
+
+def nersc_config(args, params, world):
+    return {"workload": args.workload, "lattice": "x".join(str(d) for d in params["dims"]),
+            "datatype": "4D_SU3_GAUGE_3x3", "file": "page cache (written just before the timed loads)",
+            "parallelism": f"replicas{world}", "l2": "payload 604 MB > 126 MB L2"}
+
+
+def nersc_reference_arm(args, params, rank: int, world: int):
+    """import_config_nersc restated on the host (numpy byte order and digests, the oracle's OpenMP
+    plaquette), on the same file; each step is one full load."""
+    if rank != 0:
+        return
+    import shutil
+
+    import oracle as O
+    from oracle import nersc as N
+
+    dims = params["dims"]
+    B = site_count(dims) * 4 * 9 * 16
+    d = nersc_dir(B)
+    try:
+        path = os.path.join(d, "cfg.nersc")
+        N.export_config(path, dims, O.gen_hot(dims, 1), two_row=False, beta=params["beta"])
+        for _ in range(args.warmup):
+            N.import_config(path, dims)
+        ts = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            N.import_config(path, dims)
+            ts.append(time.perf_counter() - t0)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    t = statistics.median(ts)
+    value = B / t / 1e9
+    line = {"metric": NERSC_METRIC, "value": value, "unit": "GB/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
+            "config": nersc_config(args, params, world),
+            "cpu_baseline": {"value": value, "unit": "GB/s", "cores": O.lib().mo_get_threads(), "kind": "port",
+                             "sample": "one import of the 604 MB file per step (numpy byte order, checksum, "
+                                       "zlib CRC, OpenMP plaquette)"},
+            "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_nersc(args, params, rank, world, dist):
+    import shutil
+
+    import torch
+
+    import mag_b200 as M
+
+    dims = params["dims"]
+    V = site_count(dims)
+    B = V * 4 * 9 * 16
+    seed = rank_seed(rank)
+    d = nersc_dir(2 * B)
+    path = os.path.join(d, "cfg.nersc")
+    try:
+        with M.Chmc(dims, mag=params["mag"], beta=params["beta"], n_stout=0, seed=seed) as c:
+            c.hot_start(seed)
+            c.export_config_nersc(path, skip_third=False)
+            for _ in range(args.warmup):
+                c.import_config_nersc(path)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            sampler = ClockSampler(gpu_index_for_smi()) if rank == 0 else None
+            if sampler:
+                sampler.start()
+                time.sleep(0.3)
+            t_load = []
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                c.import_config_nersc(path)
+                t_load.append(time.perf_counter() - t0)
+            t_save = []
+            for _ in range(max(1, args.steps // 2)):
+                t0 = time.perf_counter()
+                c.export_config_nersc(path + ".out", skip_third=False)
+                t_save.append(time.perf_counter() - t0)
+            kt = {k: c.time_kernel(k, 5) for k in ("nersc_swap", "nersc_crc", "nersc_to_links", "nersc_from_links",
+                                                   "nersc_plaq")}
+            torch.cuda.synchronize()
+            clocks = sampler.stop() if sampler else None
+        tl = max_over_ranks(statistics.median(t_load), dist, "cuda")
+        ts = max_over_ranks(statistics.median(t_save), dist, "cuda")
+        dev_ms = kt["nersc_swap"] + kt["nersc_crc"] + kt["nersc_to_links"] + kt["nersc_plaq"]
+        dev_ms = max_over_ranks(dev_ms, dist, "cuda")
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    if rank != 0:
+        return
+    # algorithmic HBM bytes per launch: swap reads + writes the payload, CRC reads it, the
+    # conversion reads it and writes the same bytes of link tiles
+    abytes = {"nersc_swap": 2 * B, "nersc_crc": B, "nersc_to_links": 2 * B, "nersc_from_links": 2 * B}
+    dom = max(("nersc_swap", "nersc_crc", "nersc_to_links"), key=lambda k: kt[k])
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"{args.workload}:fp64:{dom}")
+    achieved = abytes[dom] / (kt[dom] * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        import oracle as O
+        from oracle import nersc as N
+
+        d2 = nersc_dir(B)
+        try:
+            p2 = os.path.join(d2, "cfg.nersc")
+            N.export_config(p2, dims, O.gen_hot(dims, 1), two_row=False, beta=params["beta"])
+            t0 = time.perf_counter()
+            N.import_config(p2, dims)
+            tc = time.perf_counter() - t0
+        finally:
+            shutil.rmtree(d2, ignore_errors=True)
+        cpu = {"value": B / tc / 1e9, "unit": "GB/s", "cores": O.lib().mo_get_threads(), "kind": "port",
+               "sample": "one import of the same-size 3x3 file (numpy byte order, checksum, zlib CRC, OpenMP "
+                         "plaquette)"}
+    line = {
+        "metric": NERSC_METRIC, "value": world * B / (dev_ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8/f64", "data": "synthetic: Philox Haar hot start",
+        "config": nersc_config(args, params, world),
+        "value_definition": "payload bytes / device time of the load kernels (byte order + checksum, CRC-32, "
+                            "conversion to link tiles, plaquette and link-trace sums), payload already in HBM",
+        "kernel_ms": kt,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "algorithmic_bytes": abytes[dom],
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks else "fallback 6.65 TB/s"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * B / tl / 1e9, "unit": "GB/s", "h2d_bytes_per_step": B, "d2h_bytes_per_step": 0,
+                "path": "mag_gauge_load_nersc from a file in the page cache (read, copy, digests, conversion, "
+                        "plaquette check)", "ms_per_step": tl * 1e3},
+        "save_e2e": {"value": world * B / ts / 1e9, "unit": "GB/s", "d2h_bytes_per_step": B,
+                     "path": "mag_gauge_save_nersc to the page cache", "ms_per_step": ts * 1e3},
+        "clocks": clocks,
+        "gpu_launches": 7 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -467,7 +637,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     params = workload_params(args.workload)
     if args.impl == "reference":
-        reference_arm(args, params, rank, world)
+        if params.get("kind") == "nersc":
+            nersc_reference_arm(args, params, rank, world)
+        else:
+            reference_arm(args, params, rank, world)
         return
     if world > 1:
         vis = os.environ.get("CUDA_VISIBLE_DEVICES")
@@ -485,7 +658,10 @@ def main():
         dist = tdist
     torch.cuda.set_device(0)
     try:
-        run_gpu(args, params, rank, world, dist)
+        if params.get("kind") == "nersc":
+            run_nersc(args, params, rank, world, dist)
+        else:
+            run_gpu(args, params, rank, world, dist)
     finally:
         if dist:
             dist.destroy_process_group()

@@ -23,7 +23,10 @@ int mag_last_measure_ms(mag_ctx* ctx, double* ms);
 int mag_time_force(mag_ctx* ctx, int reps, double* ms_per_eval);
 /* average device time of one launch of a single kernel on the current
    fields: "force", "staple", "stout_forward", "stout_lambda", "stout_chain",
-   "evolve", "kick", "action" */
+   "evolve", "kick", "action", and the NERSC payload kernels on chain 0's
+   3x3 payload made from the current links: "nersc_swap" (byte order +
+   word checksum), "nersc_crc" (segment CRC-32), "nersc_to_links",
+   "nersc_from_links", "nersc_plaq" (plaquette and link-trace sums) */
 int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms_per_launch);
 /* re-run the launch-configuration tuner: time every register-cap variant of the
    staple / force / stout kernels on the live fields (`reps` launches each) and

@@ -171,6 +171,29 @@ inline double avg_wilson_loop(Lattice& L, const std::array<int, 3>& r, int T) {
     return v;
 }
 
+// ---------------------------------------------------- field-matrix.h NERSC I/O
+// Arg_export (field-matrix.h:445-450)
+struct Arg_export {
+    double beta = 0.0;
+    int sequence_num = 0;
+    std::string ensemble_label;
+};
+// export_config_nersc (field-matrix.h:452-572); the file is written from the device links
+inline mag_nersc_info export_config_nersc(Lattice& L, const std::string& path, const Arg_export& arg,
+                                          bool doesSkipThird = false) {
+    mag_nersc_info info;
+    check(mag_gauge_save_nersc(L.ctx(), 0, path.c_str(), doesSkipThird ? 1 : 0, arg.beta, arg.sequence_num,
+                               arg.ensemble_label.c_str(), &info),
+          "export_config_nersc");
+    return info;
+}
+// import_config_nersc (field-matrix.h:594-713); throws where the reference asserts
+inline mag_nersc_info import_config_nersc(Lattice& L, const std::string& path) {
+    mag_nersc_info info;
+    check(mag_gauge_load_nersc(L.ctx(), 0, path.c_str(), &info), "import_config_nersc");
+    return info;
+}
+
 // ------------------------------------------------------------- run_chmc
 // run_chmc (field-hmc.h:770-904): arg.num_trajectory trajectories, one summary
 // row per trajectory in the reference's format (field-hmc.h:862-864):

@@ -91,8 +91,23 @@ __global__ void k_crc32_segments(const uint8_t* p, size_t n, size_t seg, uint32_
     const size_t b1 = b0 + seg < n ? b0 + seg : n;
     uint32_t c = 0;
     size_t b = b0;
-    // segments start on multiples of 16 bytes (seg is a multiple of 16)
+    // segments start on multiples of 16 bytes (seg is a multiple of 16); four
+    // independent 16-byte loads are in flight before the table steps
     const uint4* q = reinterpret_cast<const uint4*>(p + b0);
+    for (; b + 64 <= b1; b += 64, q += 4) {
+        uint4 v[4];
+#pragma unroll
+        for (int j = 0; j < 4; j++) v[j] = q[j];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                c ^= w[k];
+                c = tab[3][c & 0xffu] ^ tab[2][(c >> 8) & 0xffu] ^ tab[1][(c >> 16) & 0xffu] ^ tab[0][c >> 24];
+            }
+        }
+    }
     for (; b + 16 <= b1; b += 16, q++) {
         const uint4 v = *q;
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
@@ -106,41 +121,66 @@ __global__ void k_crc32_segments(const uint8_t* p, size_t n, size_t seg, uint32_
     z[i] = c;
 }
 
+// Payload <-> link tiles through shared memory: a block owns 32 consecutive
+// sites (one link tile per direction); the payload of those sites is one
+// contiguous run of 32 * 4 * NC * 16 bytes, moved with coalesced 16-byte
+// accesses, while the tiles are read or written one coalesced element plane
+// at a time.  In shared memory each site's 4 * NC values are followed by one
+// pad slot, so the 32 sites of a warp start on distinct bank groups.
+constexpr int kTileSites = 32;
+constexpr int kConvThreads = 128;
+
+template <int NC>
+__device__ __forceinline__ int smem_slot(int i) {  // payload value i of the block -> shared slot
+    return i + i / (4 * NC);
+}
+
 // payload (host order) -> link tiles of one chain; NC = 6 rebuilds the third
 // row with the reference's reunitarize (field-matrix.h:83-100: CPS Unitarize
 // of rows 0, 1 unless both are zero), as import_config_nersc does after
 // copying the truncated matrices (field-matrix.h:680-690)
 template <int NC>
-__global__ void k_payload_to_links(const double* pay, int off, int V, LinkPlanes<double> U) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= V) return;
-    const int mu = blockIdx.y;
-    const double2* a = reinterpret_cast<const double2*>(pay) + ((size_t)s * 4 + mu) * NC;
+__global__ void __launch_bounds__(kConvThreads) k_payload_to_links(const double* pay, int off, int V,
+                                                                   LinkPlanes<double> U) {
+    __shared__ double2 sm[kTileSites * (4 * NC + 1)];
+    const int s0 = blockIdx.x * kTileSites;
+    const int ns = min(kTileSites, V - s0);
+    const double2* src = reinterpret_cast<const double2*>(pay) + (size_t)s0 * 4 * NC;
+    for (int i = threadIdx.x; i < ns * 4 * NC; i += kConvThreads) sm[smem_slot<NC>(i)] = src[i];
+    __syncthreads();
+    // thread = (mu, site) with the site fastest: the stores of one element are one coalesced plane
+    const int mu = threadIdx.x / kTileSites, ls = threadIdx.x % kTileSites;
+    if (ls >= ns) return;
+    const double2* a = sm + ls * (4 * NC + 1) + mu * NC;
     mat3<double> m;
     set_zero(m);
 #pragma unroll
-    for (int k = 0; k < NC; k++) {
-        const double2 v = a[k];
-        m.e[k / 3][k % 3] = mk(v.x, v.y);
-    }
+    for (int k = 0; k < NC; k++) m.e[k / 3][k % 3] = mk(a[k].x, a[k].y);
     if (NC == 6) {
         bool all_zero = true;
 #pragma unroll
         for (int k = 0; k < 6; k++) all_zero = all_zero && m.e[k / 3][k % 3].re == 0.0 && m.e[k / 3][k % 3].im == 0.0;
         if (!all_zero) unitarize(m);
     }
-    U.store(mu, off + s, m);
+    U.store(mu, off + s0 + ls, m);
 }
 
 template <int NC>
-__global__ void k_links_to_payload(LinkPlanes<double> U, int off, int V, double* pay) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= V) return;
-    const int mu = blockIdx.y;
-    const mat3<double> m = U.load(mu, off + s);
-    double2* a = reinterpret_cast<double2*>(pay) + ((size_t)s * 4 + mu) * NC;
+__global__ void __launch_bounds__(kConvThreads) k_links_to_payload(LinkPlanes<double> U, int off, int V,
+                                                                   double* pay) {
+    __shared__ double2 sm[kTileSites * (4 * NC + 1)];
+    const int s0 = blockIdx.x * kTileSites;
+    const int ns = min(kTileSites, V - s0);
+    const int mu = threadIdx.x / kTileSites, ls = threadIdx.x % kTileSites;
+    if (ls < ns) {
+        const mat3<double> m = U.load(mu, off + s0 + ls);
+        double2* a = sm + ls * (4 * NC + 1) + mu * NC;
 #pragma unroll
-    for (int k = 0; k < NC; k++) a[k] = make_double2(m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im);
+        for (int k = 0; k < NC; k++) a[k] = make_double2(m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im);
+    }
+    __syncthreads();
+    double2* dst = reinterpret_cast<double2*>(pay) + (size_t)s0 * 4 * NC;
+    for (int i = threadIdx.x; i < ns * 4 * NC; i += kConvThreads) dst[i] = sm[smem_slot<NC>(i)];
 }
 
 unsigned grid_for(size_t n, unsigned cap) {
@@ -165,15 +205,15 @@ void launch_crc32_segments(const void* payload, size_t bytes, size_t seg, uint32
 
 void launch_payload_to_links(const double* payload, int two_row, int off, int V, LinkPlanes<double> U,
                              cudaStream_t s) {
-    const dim3 grid((V + kBlock - 1) / kBlock, 4);
-    if (two_row) k_payload_to_links<6><<<grid, kBlock, 0, s>>>(payload, off, V, U);
-    else k_payload_to_links<9><<<grid, kBlock, 0, s>>>(payload, off, V, U);
+    const unsigned grid = (unsigned)((V + kTileSites - 1) / kTileSites);
+    if (two_row) k_payload_to_links<6><<<grid, kConvThreads, 0, s>>>(payload, off, V, U);
+    else k_payload_to_links<9><<<grid, kConvThreads, 0, s>>>(payload, off, V, U);
 }
 
 void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s) {
-    const dim3 grid((V + kBlock - 1) / kBlock, 4);
-    if (two_row) k_links_to_payload<6><<<grid, kBlock, 0, s>>>(U, off, V, payload);
-    else k_links_to_payload<9><<<grid, kBlock, 0, s>>>(U, off, V, payload);
+    const unsigned grid = (unsigned)((V + kTileSites - 1) / kTileSites);
+    if (two_row) k_links_to_payload<6><<<grid, kConvThreads, 0, s>>>(U, off, V, payload);
+    else k_links_to_payload<9><<<grid, kConvThreads, 0, s>>>(U, off, V, payload);
 }
 
 }  // namespace magb

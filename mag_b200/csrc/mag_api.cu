@@ -6,6 +6,8 @@
 // trajectory (momenta, H_old, integration, reunitarisation, H_new, accept,
 // restore, record) replays as a single CUDA graph with no host round trip.
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cmath>
@@ -13,6 +15,7 @@
 #include <functional>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mag_c.h"
@@ -951,6 +954,13 @@ int mag_time_force(mag_ctx* ctx, int reps, double* ms) {
     return MAG_OK;
 }
 
+}  // extern "C"
+namespace {
+constexpr size_t kCrcSeg = 4096;  // bytes per CRC segment register (NERSC digests)
+int nersc_buffers(mag_ctx* ctx);
+}  // namespace
+extern "C" {
+
 int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms) {
     if (!ctx || !which || !ms || reps < 1) return MAG_ERR_ARG;
     const std::string w(which);
@@ -973,7 +983,29 @@ int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms) {
         return ctx->time_one<double>(f, ctx->var<double>(f), reps, ctx->st64, ctx->U, ctx->F, ctx->Uaux, ms);
     }
     std::function<void()> fn;
-    if (w == "evolve") {
+    if (w.rfind("nersc_", 0) == 0) {
+        // NERSC payload kernels on chain 0's full (3x3) payload, made from the current links
+        MAG_TRY(nersc_buffers(ctx));
+        const ChainInfo& c0 = ctx->hc[0];
+        const size_t bytes = (size_t)c0.V * 4 * 9 * 16;
+        launch_links_to_payload(ctx->U, 0, c0.off, c0.V, ctx->staging, s);
+        if (w == "nersc_swap") {
+            fn = [&]() { launch_swap64_sum32(ctx->staging, bytes, true, ctx->d_csum, s); };
+        } else if (w == "nersc_crc") {
+            fn = [&]() { launch_crc32_segments(ctx->staging, bytes, kCrcSeg, ctx->d_crc, s); };
+        } else if (w == "nersc_to_links") {  // rewrites the same links bit for bit
+            fn = [&]() { launch_payload_to_links(ctx->staging, 0, c0.off, c0.V, ctx->U, s); };
+        } else if (w == "nersc_from_links") {
+            fn = [&]() { launch_links_to_payload(ctx->U, 0, c0.off, c0.V, ctx->staging, s); };
+        } else if (w == "nersc_plaq") {  // the plaquette and link-trace sums of the import check
+            fn = [&]() {
+                launch_action_sums<double>(g, ctx->U, false, ctx->partial, ctx->sums, SLOT_SCRATCH, SLOT_SCRATCH, s);
+                launch_link_trace_sum(g, ctx->U, ctx->partial, ctx->sums, SLOT_SCRATCH2, s);
+            };
+        } else {
+            return fail(MAG_ERR_ARG, "mag_time_kernel: unknown kernel '" + w + "'");
+        }
+    } else if (w == "evolve") {
         fn = [&]() {
             launch_evolve<double, double>(g, ctx->U, ctx->Ubak, ctx->P, 1e-3,
                                           m ? ctx->Uaux32 : LinkPlanes<float>{nullptr, 0}, s);
@@ -1167,8 +1199,13 @@ int mag_constrained_plaquette(mag_ctx* ctx, int chain, double* out) {
 // ------------------------------------------------------------- NERSC I/O
 namespace {
 
-constexpr size_t kCrcSeg = 16384;          // bytes per CRC segment register
-constexpr size_t kIoChunk = 64u << 20;     // pinned chunk of the file <-> device copies
+constexpr size_t kIoChunk = 8u << 20;      // pinned chunk of the file <-> device copies
+
+// reader / writer threads of the file <-> device pipeline (two pinned slots each)
+int io_threads() {
+    const unsigned hc = std::thread::hardware_concurrency();
+    return (int)std::max(2u, std::min(8u, hc / 2));
+}
 
 void fill_info(mag_nersc_info* info, const nersc::Header& h, int two_row) {
     memset(info, 0, sizeof(*info));
@@ -1190,7 +1227,7 @@ struct FileCloser {
 
 int nersc_buffers(mag_ctx* ctx) {
     std::string err;
-    int r = ctx->pin.ensure(kIoChunk, err);
+    int r = ctx->pin.ensure(2 * io_threads(), kIoChunk, err);
     if (r != MAG_OK) return fail(r, err);
     if (!ctx->d_crc) {
         const size_t nseg = (sizeof(double) * 72 * (size_t)ctx->max_v + kCrcSeg - 1) / kCrcSeg;
@@ -1272,9 +1309,8 @@ int mag_gauge_load_nersc(mag_ctx* ctx, int chain, const char* path, mag_nersc_in
                                             std::to_string(h.dims[3]) + ")");
     MAG_TRY(nersc_buffers(ctx));
     const size_t bytes = (size_t)ci.V * 4 * (two_row ? 6 : 9) * 16;
-    if (fseeko(fc.f, (off_t)h.payload_offset, SEEK_SET) != 0)
-        return fail(MAG_ERR_IO, "import_config_nersc: cannot seek to the payload");
-    r = nersc::file_to_device(fc.f, ctx->staging, bytes, ctx->pin, ctx->stream, err);
+    r = nersc::file_to_device(fileno(fc.f), h.payload_offset, ctx->staging, bytes, ctx->pin, io_threads(),
+                              ctx->stream, err);
     if (r != MAG_OK) return fail(r, "import_config_nersc: " + err);
     uint32_t crc = 0, csum = 0;
     MAG_TRY(payload_digest(ctx, bytes, true, &crc, &csum));
@@ -1320,15 +1356,22 @@ int mag_gauge_save_nersc(mag_ctx* ctx, int chain, const char* path, int two_row,
     MAG_TRY(payload_digest(ctx, bytes, false, &crc, &csum));
     const std::string hdr = nersc::format_header(ci.L, two_row ? 1 : 0, crc, csum, trace, plaq, ensemble_label,
                                                  sequence_number, beta, (long long)time(nullptr));
-    FileCloser fc{fopen(path, "wb")};
-    if (!fc.f) return fail(MAG_ERR_IO, std::string("cannot create ") + path);
-    if (fputs(hdr.c_str(), fc.f) < 0) return fail(MAG_ERR_IO, "export_config_nersc: header write failed");
+    const int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) return fail(MAG_ERR_IO, std::string("cannot create ") + path);
     std::string err;
-    const int r = nersc::device_to_file(ctx->staging, bytes, fc.f, ctx->pin, ctx->stream, err);
+    int r = MAG_OK;
+    if (pwrite(fd, hdr.data(), hdr.size(), 0) != (ssize_t)hdr.size()) {
+        r = MAG_ERR_IO;
+        err = "header write failed";
+    }
+    if (r == MAG_OK)
+        r = nersc::device_to_file(ctx->staging, bytes, fd, (long long)hdr.size(), ctx->pin, io_threads(),
+                                  ctx->stream, err);
+    if (close(fd) != 0 && r == MAG_OK) {
+        r = MAG_ERR_IO;
+        err = "close failed";
+    }
     if (r != MAG_OK) return fail(r, "export_config_nersc: " + err);
-    const int cl = fclose(fc.f);
-    fc.f = nullptr;
-    if (cl != 0) return fail(MAG_ERR_IO, "export_config_nersc: close failed");
     if (info) {
         memset(info, 0, sizeof(*info));
         for (int d = 0; d < 4; d++) info->dims[d] = ci.L[d];

@@ -1,9 +1,17 @@
 // nersc_host.cpp -- host side of NERSC configuration I/O (see nersc_host.h).
 #include "nersc_host.h"
 
+#include <errno.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <condition_variable>
+#include <mutex>
+#include <thread>
+#include <vector>
 
 #include "../../include/mag_c.h"
 
@@ -202,10 +210,11 @@ uint32_t crc32_chain(const uint32_t* z, size_t nseg, size_t seg, size_t total) {
     return ~r;
 }
 
-int Pinned::ensure(size_t chunk_bytes, std::string& err) {
-    if (buf[0] && chunk >= chunk_bytes) return MAG_OK;
+int Pinned::ensure(int nslots, size_t chunk_bytes, std::string& err) {
+    if (nslots > kMaxSlots) nslots = kMaxSlots;
+    if (slots >= nslots && chunk >= chunk_bytes) return MAG_OK;
     release();
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < nslots; i++) {
         if (cudaHostAlloc(&buf[i], chunk_bytes, cudaHostAllocDefault) != cudaSuccess ||
             cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) {
             cudaGetLastError();
@@ -213,77 +222,168 @@ int Pinned::ensure(size_t chunk_bytes, std::string& err) {
             err = "cannot allocate pinned staging buffers";
             return MAG_ERR_NOMEM;
         }
+        slots = i + 1;
     }
     chunk = chunk_bytes;
     return MAG_OK;
 }
 
 void Pinned::release() {
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kMaxSlots; i++) {
         if (buf[i]) cudaFreeHost(buf[i]);
         if (ev[i]) cudaEventDestroy(ev[i]);
         buf[i] = nullptr;
         ev[i] = nullptr;
     }
+    slots = 0;
     chunk = 0;
 }
 
-int file_to_device(FILE* f, void* d, size_t bytes, Pinned& pin, cudaStream_t stream, std::string& err) {
-    // chunk k is read into buffer k % 2 once the copy of chunk k - 2 out of it has finished
-    size_t done = 0;
-    for (int k = 0; done < bytes; k++) {
-        const int i = k & 1;
-        const size_t n = bytes - done < pin.chunk ? bytes - done : pin.chunk;
-        if (k >= 2 && cudaEventSynchronize(pin.ev[i]) != cudaSuccess) {
-            err = "cudaEventSynchronize failed";
-            return MAG_ERR_CUDA;
+namespace {
+
+// Ordered chunk pipeline over the pinned ring.  Chunk i uses slot i % K.
+// Reading: worker (i mod T) preads chunk i once the copy of chunk i - K out
+// of the slot has completed; the caller issues the copies in chunk order.
+// Writing: the caller issues the copy of chunk i into its slot once chunk
+// i - K has been written; worker (i mod T) pwrites chunk i after its copy.
+class Pipeline {
+  public:
+    Pipeline(Pinned& pin, size_t bytes, int threads, bool to_device)
+        : pin_(pin), bytes_(bytes), to_device_(to_device) {
+        n_ = (long)((bytes + pin.chunk - 1) / pin.chunk);
+        T_ = std::max(1, std::min(threads, pin.slots / 2));
+        K_ = std::min(pin.slots, 2 * T_);
+        for (int k = 0; k < K_; k++) {
+            filled_[k] = -1;
+            copied_[k] = -1;
         }
-        if (fread(pin.buf[i], 1, n, f) != n) {
-            err = "payload shorter than the lattice needs";
-            return MAG_ERR_FORMAT;
-        }
-        if (cudaMemcpyAsync(static_cast<char*>(d) + done, pin.buf[i], n, cudaMemcpyHostToDevice, stream) !=
-                cudaSuccess ||
-            cudaEventRecord(pin.ev[i], stream) != cudaSuccess) {
-            err = "host to device copy failed";
-            return MAG_ERR_CUDA;
-        }
-        done += n;
     }
-    if (cudaStreamSynchronize(stream) != cudaSuccess) {
-        err = "host to device copy failed";
-        return MAG_ERR_CUDA;
+
+    int run(int fd, long long off, char* dev, cudaStream_t stream, std::string& err) {
+        std::vector<std::thread> workers;
+        for (int t = 0; t < T_; t++) workers.emplace_back([=] { worker(t, fd, off); });
+        int rc = MAG_OK;
+        for (long i = 0; i < n_ && rc == MAG_OK; i++) {
+            const int k = (int)(i % K_);
+            const size_t len = size_of(i);
+            if (to_device_) {
+                if (!wait_until([&] { return filled_[k] >= i; })) break;  // chunk i in the slot
+                if (cudaMemcpyAsync(dev + i * pin_.chunk, pin_.buf[k], len, cudaMemcpyHostToDevice, stream) !=
+                        cudaSuccess ||
+                    cudaEventRecord(pin_.ev[k], stream) != cudaSuccess)
+                    rc = fail_all(MAG_ERR_CUDA, "host to device copy failed");
+            } else {
+                if (!wait_until([&] { return filled_[k] >= i - K_; })) break;  // chunk i - K written out
+                if (cudaMemcpyAsync(pin_.buf[k], dev + i * pin_.chunk, len, cudaMemcpyDeviceToHost, stream) !=
+                        cudaSuccess ||
+                    cudaEventRecord(pin_.ev[k], stream) != cudaSuccess)
+                    rc = fail_all(MAG_ERR_CUDA, "device to host copy failed");
+            }
+            if (rc == MAG_OK) {
+                std::lock_guard<std::mutex> g(m_);
+                copied_[k] = i;
+                cv_.notify_all();
+            }
+        }
+        for (auto& w : workers) w.join();
+        if (rc == MAG_OK && to_device_ && cudaStreamSynchronize(stream) != cudaSuccess)
+            rc = fail_all(MAG_ERR_CUDA, "host to device copy failed");
+        if (rc == MAG_OK && rc_ != MAG_OK) rc = rc_;
+        if (rc != MAG_OK) err = msg_;
+        return rc;
     }
-    return MAG_OK;
+
+  private:
+    size_t size_of(long i) const { return i + 1 < n_ ? pin_.chunk : bytes_ - (size_t)i * pin_.chunk; }
+
+    template <typename Pred>
+    bool wait_until(Pred p) {
+        std::unique_lock<std::mutex> g(m_);
+        cv_.wait(g, [&] { return p() || rc_ != MAG_OK; });
+        return rc_ == MAG_OK;
+    }
+
+    int fail_all(int rc, const char* msg) {
+        std::lock_guard<std::mutex> g(m_);
+        if (rc_ == MAG_OK) {
+            rc_ = rc;
+            msg_ = msg;
+        }
+        cv_.notify_all();
+        return rc;
+    }
+
+    void worker(int t, int fd, long long off) {
+        for (long i = t; i < n_; i += T_) {
+            const int k = (int)(i % K_);
+            if (to_device_) {
+                // the copy of chunk i - K out of this slot was issued; wait for it to finish
+                if (i >= K_) {
+                    if (!wait_until([&] { return copied_[k] >= i - K_; })) return;
+                    if (cudaEventSynchronize(pin_.ev[k]) != cudaSuccess) {
+                        fail_all(MAG_ERR_CUDA, "cudaEventSynchronize failed");
+                        return;
+                    }
+                }
+                if (!xfer(fd, off + (long long)i * (long long)pin_.chunk, pin_.buf[k], size_of(i), true)) return;
+            } else {
+                if (!wait_until([&] { return copied_[k] >= i; })) return;
+                if (cudaEventSynchronize(pin_.ev[k]) != cudaSuccess) {
+                    fail_all(MAG_ERR_CUDA, "cudaEventSynchronize failed");
+                    return;
+                }
+                if (!xfer(fd, off + (long long)i * (long long)pin_.chunk, pin_.buf[k], size_of(i), false)) return;
+            }
+            std::lock_guard<std::mutex> g(m_);
+            filled_[k] = i;
+            cv_.notify_all();
+        }
+    }
+
+    bool xfer(int fd, long long pos, void* b, size_t len, bool read) {
+        char* p = static_cast<char*>(b);
+        while (len) {
+            const ssize_t r = read ? pread(fd, p, len, (off_t)pos) : pwrite(fd, p, len, (off_t)pos);
+            if (r < 0 && errno == EINTR) continue;
+            if (r <= 0) {
+                if (read && r == 0) fail_all(MAG_ERR_FORMAT, "payload shorter than the lattice needs");
+                else fail_all(MAG_ERR_IO, read ? "read failed" : "write failed");
+                return false;
+            }
+            p += r;
+            pos += r;
+            len -= (size_t)r;
+        }
+        return true;
+    }
+
+    Pinned& pin_;
+    size_t bytes_;
+    bool to_device_;
+    long n_ = 0;
+    int T_ = 1, K_ = 2;
+    long filled_[Pinned::kMaxSlots];  // reading: chunk now in the slot; writing: chunk written from it
+    long copied_[Pinned::kMaxSlots];  // last chunk whose device copy was issued on the slot
+    std::mutex m_;
+    std::condition_variable cv_;
+    int rc_ = MAG_OK;
+    std::string msg_;
+};
+
+}  // namespace
+
+int file_to_device(int fd, long long off, void* d, size_t bytes, Pinned& pin, int threads, cudaStream_t stream,
+                   std::string& err) {
+    if (bytes == 0) return MAG_OK;
+    Pipeline p(pin, bytes, threads, true);
+    return p.run(fd, off, static_cast<char*>(d), stream, err);
 }
 
-int device_to_file(const void* d, size_t bytes, FILE* f, Pinned& pin, cudaStream_t stream, std::string& err) {
-    // the copy of chunk k overlaps the write of chunk k - 1
-    const size_t nchunk = (bytes + pin.chunk - 1) / pin.chunk;
-    auto size_of = [&](size_t k) { return k + 1 < nchunk ? pin.chunk : bytes - k * pin.chunk; };
-    for (size_t k = 0; k <= nchunk; k++) {
-        if (k < nchunk) {
-            const int i = (int)(k & 1);
-            if (cudaMemcpyAsync(pin.buf[i], static_cast<const char*>(d) + k * pin.chunk, size_of(k),
-                                cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-                cudaEventRecord(pin.ev[i], stream) != cudaSuccess) {
-                err = "device to host copy failed";
-                return MAG_ERR_CUDA;
-            }
-        }
-        if (k >= 1) {
-            const int j = (int)((k - 1) & 1);
-            if (cudaEventSynchronize(pin.ev[j]) != cudaSuccess) {
-                err = "device to host copy failed";
-                return MAG_ERR_CUDA;
-            }
-            if (fwrite(pin.buf[j], 1, size_of(k - 1), f) != size_of(k - 1)) {
-                err = "write failed";
-                return MAG_ERR_IO;
-            }
-        }
-    }
-    return MAG_OK;
+int device_to_file(const void* d, size_t bytes, int fd, long long off, Pinned& pin, int threads,
+                   cudaStream_t stream, std::string& err) {
+    if (bytes == 0) return MAG_OK;
+    Pipeline p(pin, bytes, threads, false);
+    return p.run(fd, off, const_cast<char*>(static_cast<const char*>(d)), stream, err);
 }
 
 }  // namespace nersc

@@ -53,20 +53,27 @@ uint32_t crc32_chain(const uint32_t* z, size_t nseg, size_t seg, size_t total);
 // register of one segment on the host (same definition as the device kernel)
 uint32_t crc32_register(const uint8_t* p, size_t n);
 
-// Pinned double buffer for chunked copies between a file and device memory.
+// Pinned ring of chunk buffers for pipelined copies between a file and
+// device memory: reader/writer threads move chunks between the file (pread /
+// pwrite, page cache) and the ring while the calling thread issues the
+// host<->device copies in order on the stream.
 struct Pinned {
-    void* buf[2] = {nullptr, nullptr};
-    cudaEvent_t ev[2] = {nullptr, nullptr};
+    static constexpr int kMaxSlots = 32;
+    void* buf[kMaxSlots] = {};
+    cudaEvent_t ev[kMaxSlots] = {};
+    int slots = 0;
     size_t chunk = 0;
-    int ensure(size_t chunk_bytes, std::string& err);
+    int ensure(int nslots, size_t chunk_bytes, std::string& err);
     void release();
 };
 
-// read `bytes` from f (positioned at the payload) into device memory d
-// through the pinned buffers on `stream`; returns MAG_OK / MAG_ERR_IO / MAG_ERR_CUDA
-int file_to_device(FILE* f, void* d, size_t bytes, Pinned& pin, cudaStream_t stream, std::string& err);
-// write `bytes` of device memory d to f after the header
-int device_to_file(const void* d, size_t bytes, FILE* f, Pinned& pin, cudaStream_t stream, std::string& err);
+// file (descriptor fd, payload at byte offset off) -> device memory d, with
+// `threads` reader threads; MAG_OK / MAG_ERR_IO / MAG_ERR_FORMAT (short file) / MAG_ERR_CUDA
+int file_to_device(int fd, long long off, void* d, size_t bytes, Pinned& pin, int threads, cudaStream_t stream,
+                   std::string& err);
+// device memory d -> file at byte offset off, with `threads` writer threads
+int device_to_file(const void* d, size_t bytes, int fd, long long off, Pinned& pin, int threads,
+                   cudaStream_t stream, std::string& err);
 
 }  // namespace nersc
 }  // namespace magb

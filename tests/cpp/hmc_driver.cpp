@@ -24,9 +24,22 @@ int main(int argc, char** argv) {
         const double h = mag_b200::get_hamiltonian(lat, part);
         auto res = mag_b200::run_chmc(lat, stderr);
         const double c1 = mag_b200::check_constrained_plaquette(lat);
+        // save the configuration and resume from it in a second lattice (quench_test/main.C:92-106)
+        double plaq_reload = 0.0;
+        if (argc > 2) {
+            mag_b200::Arg_export ax;
+            ax.beta = arg.beta;
+            ax.sequence_num = 3;
+            ax.ensemble_label = "cpp_driver";
+            mag_b200::export_config_nersc(lat, argv[2], ax, true);
+            mag_b200::Lattice lat2({L, L, L, 2 * L}, arg, opt);
+            mag_b200::import_config_nersc(lat2, argv[2]);
+            plaq_reload = mag_b200::avg_plaquette(lat2);
+        }
         std::printf("{\"h0\": %.17g, \"kin0\": %.17g, \"dh\": [%.17g, %.17g, %.17g], \"plaq\": %.17g, "
-                    "\"cplaq_before\": %.17g, \"cplaq_after\": %.17g}\n",
-                    h, part[0], res[0].delta_h, res[1].delta_h, res[2].delta_h, mag_b200::avg_plaquette(lat), c0, c1);
+                    "\"cplaq_before\": %.17g, \"cplaq_after\": %.17g, \"plaq_reload\": %.17g}\n",
+                    h, part[0], res[0].delta_h, res[1].delta_h, res[2].delta_h, mag_b200::avg_plaquette(lat), c0, c1,
+                    plaq_reload);
     } catch (const mag_b200::Error& e) {
         std::fprintf(stderr, "error %d: %s\n", e.code, e.what());
         return 2;

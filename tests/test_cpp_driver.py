@@ -25,10 +25,11 @@ def test_cpp_driver_compiles_and_links():
 
 
 @pytest.mark.gpu
-def test_cpp_driver_matches_python_api():
+def test_cpp_driver_matches_python_api(tmp_path):
     import mag_b200 as M
 
-    out = subprocess.run([build_driver(), "4"], check=True, capture_output=True, text=True)
+    out = subprocess.run([build_driver(), "4", str(tmp_path / "cfg.nersc")], check=True, capture_output=True,
+                         text=True)
     res = json.loads(out.stdout.strip().splitlines()[-1])
     with M.Chmc((4, 4, 4, 8), mag=2, n_stout=1, rho=0.1, n_steps=4, tau=1.0, seed=5) as c:
         c.hot_start(3)
@@ -37,3 +38,5 @@ def test_cpp_driver_matches_python_api():
     assert res["h0"] == H and res["kin0"] == parts[0]
     assert res["dh"] == [r[0]["delta_h"] for r in recs]
     assert abs(res["cplaq_after"] - res["cplaq_before"]) < 1e-12
+    # export_config_nersc -> import_config_nersc (two-row file, third row rebuilt) resumes the same field
+    assert abs(res["plaq_reload"] - res["plaq"]) < 1e-13

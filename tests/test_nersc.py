@@ -204,12 +204,13 @@ def test_load_errors(tmp_path):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("two_row", [True, False])
-def test_roundtrip_full_size(tmp_path, two_row):
-    """16^3 x 32 (payload 50-75 MB, more than one pinned chunk of the CRC
-    segments): save -> load is exact (3x3) or a fixed point of reunitarize
-    (two-row), and the file's digests equal zlib / numpy over the payload."""
-    dims = (16, 16, 16, 32)
+@pytest.mark.parametrize("two_row,dims", [(True, (16, 16, 16, 32)), (False, (16, 16, 16, 32)),
+                                          (False, (24, 24, 24, 24))])
+def test_roundtrip_full_size(tmp_path, two_row, dims):
+    """16^3 x 32 and 24^4 (payload 50-191 MB: many 8 MB pipeline chunks, the
+    24^4 file more chunks than pinned slots, so every slot is reused):
+    save -> load is exact (3x3) or a fixed point of reunitarize (two-row), and
+    the file's digests equal zlib / numpy over the payload."""
     p = tmp_path / "big"
     with M.Chmc(dims, seed=2) as c:
         c.hot_start(4)
