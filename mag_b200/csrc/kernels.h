@@ -145,6 +145,9 @@ void launch_swap64_sum32(void* payload, size_t bytes, bool to_host, unsigned int
 // z[i] = CRC-32 register (zlib polynomial, zero start, no final complement) of bytes [i*seg, (i+1)*seg)
 // of the payload; seg a multiple of 16
 void launch_crc32_segments(const void* payload, size_t bytes, size_t seg, uint32_t* z, cudaStream_t s);
+// z2[g] = fold of z[g*G .. (g+1)*G) (n registers of equal-length segments) with the one-segment zero-byte
+// advance given as four 256-entry byte tables in device memory (tab[k * 256 + b])
+void launch_crc32_fold(const uint32_t* z, size_t n, int G, const uint32_t* tab, uint32_t* z2, cudaStream_t s);
 // host-order payload <-> links of the chain at site offset off (two_row: 6 complex per link, third row
 // rebuilt by reunitarize; else 9)
 void launch_payload_to_links(const double* payload, int two_row, int off, int V, LinkPlanes<double> U,

@@ -121,6 +121,23 @@ __global__ void k_crc32_segments(const uint8_t* p, size_t n, size_t seg, uint32_
     z[i] = c;
 }
 
+// z2[g] = fold of the registers z[g*G .. min((g+1)*G, n)) of consecutive
+// equal-length segments: r <- S(r) ^ z[j] from r = 0, S the register advance
+// over one segment of zero bytes given as four byte tables (tab[k][b])
+__global__ void k_crc32_fold(const uint32_t* z, size_t n, int G, const uint32_t* tab, uint32_t* z2, size_t ngroups) {
+    __shared__ uint32_t t[4][256];
+    for (int i = threadIdx.x; i < 4 * 256; i += blockDim.x) t[i >> 8][i & 255] = tab[i];
+    __syncthreads();
+    const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= ngroups) return;
+    const size_t j0 = g * (size_t)G;
+    const size_t j1 = j0 + G < n ? j0 + G : n;
+    uint32_t r = 0;
+    for (size_t j = j0; j < j1; j++)
+        r = t[0][r & 0xffu] ^ t[1][(r >> 8) & 0xffu] ^ t[2][(r >> 16) & 0xffu] ^ t[3][r >> 24] ^ z[j];
+    z2[g] = r;
+}
+
 // Payload <-> link tiles through shared memory: a block owns 32 consecutive
 // sites (one link tile per direction); the payload of those sites is one
 // contiguous run of 32 * 4 * NC * 16 bytes, moved with coalesced 16-byte
@@ -201,6 +218,12 @@ void launch_crc32_segments(const void* payload, size_t bytes, size_t seg, uint32
     const size_t nseg = (bytes + seg - 1) / seg;
     k_crc32_segments<<<grid_for(nseg, 1u << 30), kBlock, 0, s>>>(static_cast<const uint8_t*>(payload), bytes, seg,
                                                                  z, nseg);
+}
+
+void launch_crc32_fold(const uint32_t* z, size_t n, int G, const uint32_t* tab, uint32_t* z2, cudaStream_t s) {
+    const size_t ng = (n + G - 1) / G;
+    if (ng == 0) return;
+    k_crc32_fold<<<grid_for(ng, 1u << 30), kBlock, 0, s>>>(z, n, G, tab, z2, ng);
 }
 
 void launch_payload_to_links(const double* payload, int two_row, int off, int V, LinkPlanes<double> U,

@@ -119,7 +119,10 @@ struct mag_ctx {
     long max_v = 0;
     // NERSC I/O: pinned double buffer, CRC segment registers, word checksum
     nersc::Pinned pin;
-    uint32_t* d_crc = nullptr;
+    uint32_t* d_crc = nullptr;      // segment registers (kCrcThreads + 1)
+    uint32_t* d_crc2 = nullptr;     // folded groups
+    uint32_t* d_crc_tab = nullptr;  // 4 x 256 shift tables of one segment
+    size_t crc_tab_seg = 0;         // segment length the tables hold
     unsigned int* d_csum = nullptr;
     long long host_traj = 0;
     cudaGraphExec_t graph = nullptr;
@@ -956,8 +959,15 @@ int mag_time_force(mag_ctx* ctx, int reps, double* ms) {
 
 }  // extern "C"
 namespace {
-constexpr size_t kCrcSeg = 4096;  // bytes per CRC segment register (NERSC digests)
+// CRC segments: about two per resident thread of a 148-SM device, at least 256 bytes each
+constexpr size_t kCrcThreads = 148 * 2048 * 2;
+constexpr int kCrcGroup = 64;  // segment registers folded per thread on the device
+size_t crc_seg(size_t bytes) {
+    const size_t s = (bytes + kCrcThreads - 1) / kCrcThreads;
+    return std::max<size_t>(256, (s + 15) / 16 * 16);
+}
 int nersc_buffers(mag_ctx* ctx);
+int ensure_crc_tab(mag_ctx* ctx, size_t seg);
 }  // namespace
 extern "C" {
 
@@ -992,7 +1002,12 @@ int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms) {
         if (w == "nersc_swap") {
             fn = [&]() { launch_swap64_sum32(ctx->staging, bytes, true, ctx->d_csum, s); };
         } else if (w == "nersc_crc") {
-            fn = [&]() { launch_crc32_segments(ctx->staging, bytes, kCrcSeg, ctx->d_crc, s); };
+            const size_t seg = crc_seg(bytes);
+            MAG_TRY(ensure_crc_tab(ctx, seg));
+            fn = [&, seg]() {
+                launch_crc32_segments(ctx->staging, bytes, seg, ctx->d_crc, s);
+                launch_crc32_fold(ctx->d_crc, bytes / seg, kCrcGroup, ctx->d_crc_tab, ctx->d_crc2, s);
+            };
         } else if (w == "nersc_to_links") {  // rewrites the same links bit for bit
             fn = [&]() { launch_payload_to_links(ctx->staging, 0, c0.off, c0.V, ctx->U, s); };
         } else if (w == "nersc_from_links") {
@@ -1230,8 +1245,9 @@ int nersc_buffers(mag_ctx* ctx) {
     int r = ctx->pin.ensure(2 * io_threads(), kIoChunk, err);
     if (r != MAG_OK) return fail(r, err);
     if (!ctx->d_crc) {
-        const size_t nseg = (sizeof(double) * 72 * (size_t)ctx->max_v + kCrcSeg - 1) / kCrcSeg;
-        MAG_TRY(ctx->alloc((void**)&ctx->d_crc, sizeof(uint32_t) * nseg));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_crc, sizeof(uint32_t) * (kCrcThreads + 1)));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_crc2, sizeof(uint32_t) * (kCrcThreads / kCrcGroup + 1)));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_crc_tab, sizeof(uint32_t) * 4 * 256));
         MAG_TRY(ctx->alloc((void**)&ctx->d_csum, sizeof(unsigned int)));
     }
     return MAG_OK;
@@ -1255,19 +1271,44 @@ int plaq_and_trace(mag_ctx* ctx, int chain, double* plaq, double* trace) {
 // CRC-32 of the host-order payload in staging and its 32-bit word sum; to_be
 // leaves the payload big-endian (export), else it is converted to host order
 // first (import)
+int ensure_crc_tab(mag_ctx* ctx, size_t seg) {
+    if (ctx->crc_tab_seg == seg) return MAG_OK;
+    uint32_t tab[4][256];
+    nersc::crc32_shift_tables(seg, tab);
+    MAG_CUDA(cudaMemcpy(ctx->d_crc_tab, tab, sizeof(tab), cudaMemcpyHostToDevice));
+    ctx->crc_tab_seg = seg;
+    return MAG_OK;
+}
+
 int payload_digest(mag_ctx* ctx, size_t bytes, bool import, uint32_t* crc, uint32_t* csum) {
-    const size_t nseg = (bytes + kCrcSeg - 1) / kCrcSeg;
+    const size_t seg = crc_seg(bytes);
+    const size_t nfull = bytes / seg, tail = bytes - nfull * seg;
+    const size_t ngroups = (nfull + kCrcGroup - 1) / kCrcGroup;
+    MAG_TRY(ensure_crc_tab(ctx, seg));
     MAG_CUDA(cudaMemsetAsync(ctx->d_csum, 0, sizeof(unsigned int), ctx->stream));
     if (import) launch_swap64_sum32(ctx->staging, bytes, true, ctx->d_csum, ctx->stream);
-    launch_crc32_segments(ctx->staging, bytes, kCrcSeg, ctx->d_crc, ctx->stream);
+    launch_crc32_segments(ctx->staging, bytes, seg, ctx->d_crc, ctx->stream);
+    launch_crc32_fold(ctx->d_crc, nfull, kCrcGroup, ctx->d_crc_tab, ctx->d_crc2, ctx->stream);
     if (!import) launch_swap64_sum32(ctx->staging, bytes, false, ctx->d_csum, ctx->stream);
     MAG_TRY(ctx->check("NERSC payload digest"));
-    std::vector<uint32_t> z(nseg);
+    std::vector<uint32_t> z2(ngroups + 1);
     unsigned int sum = 0;
-    MAG_CUDA(cudaMemcpyAsync(z.data(), ctx->d_crc, sizeof(uint32_t) * nseg, cudaMemcpyDeviceToHost, ctx->stream));
+    if (ngroups)
+        MAG_CUDA(cudaMemcpyAsync(z2.data(), ctx->d_crc2, sizeof(uint32_t) * ngroups, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    if (tail)
+        MAG_CUDA(cudaMemcpyAsync(&z2[ngroups], ctx->d_crc + nfull, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
     MAG_CUDA(cudaMemcpyAsync(&sum, ctx->d_csum, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
     MAG_TRY(ctx->sync("NERSC payload digest"));
-    *crc = nersc::crc32_chain(z.data(), nseg, kCrcSeg, bytes);
+    // zlib: register started at ~0, result complemented; groups of kCrcGroup segments, the last group shorter
+    uint32_t r = 0xFFFFFFFFu;
+    if (ngroups) {
+        const size_t last = (nfull - (ngroups - 1) * kCrcGroup) * seg;
+        r = nersc::crc32_fold(r, z2.data(), ngroups, kCrcGroup * seg, last);
+    }
+    if (tail) r = nersc::crc32_fold(r, &z2[ngroups], 1, tail, tail);
+    *crc = ~r;
     *csum = sum;
     return MAG_OK;
 }

@@ -199,15 +199,23 @@ uint32_t crc32_register(const uint8_t* p, size_t n) {
     return c;
 }
 
+void crc32_shift_tables(size_t nbytes, uint32_t t[4][256]) {
+    const ByteTables b(zero_bytes(nbytes));
+    memcpy(t, b.t, sizeof(b.t));
+}
+
+uint32_t crc32_fold(uint32_t r, const uint32_t* z, size_t n, size_t len_each, size_t len_last) {
+    // register(R, A||B) = S_|B|(register(R, A)) ^ register(0, B)
+    if (n == 0) return r;
+    const ByteTables each(zero_bytes(len_each));
+    for (size_t i = 0; i + 1 < n; i++) r = each(r) ^ z[i];
+    return (len_last == len_each ? each(r) : ByteTables(zero_bytes(len_last))(r)) ^ z[n - 1];
+}
+
 uint32_t crc32_chain(const uint32_t* z, size_t nseg, size_t seg, size_t total) {
-    // register(R, A||B) = shift_|B|(register(R, A)) ^ register(0, B); zlib starts at ~0 and complements
-    uint32_t r = 0xFFFFFFFFu;
-    if (nseg == 0) return ~r;
-    const ByteTables full(zero_bytes(seg));
-    for (size_t i = 0; i + 1 < nseg; i++) r = full(r) ^ z[i];
-    const size_t last = total - (nseg - 1) * seg;
-    r = (last == seg ? full(r) : ByteTables(zero_bytes(last))(r)) ^ z[nseg - 1];
-    return ~r;
+    // zlib starts the register at ~0 and complements the result
+    if (nseg == 0) return 0u;
+    return ~crc32_fold(0xFFFFFFFFu, z, nseg, seg, total - (nseg - 1) * seg);
 }
 
 int Pinned::ensure(int nslots, size_t chunk_bytes, std::string& err) {

@@ -52,6 +52,10 @@ std::string format_header(const int dims[4], int two_row, uint32_t crc32, uint32
 uint32_t crc32_chain(const uint32_t* z, size_t nseg, size_t seg, size_t total);
 // register of one segment on the host (same definition as the device kernel)
 uint32_t crc32_register(const uint8_t* p, size_t n);
+// register advance over n zero bytes as four byte tables: S_n(v) = t[0][v & 255] ^ t[1][(v >> 8) & 255] ^ ...
+void crc32_shift_tables(size_t nbytes, uint32_t t[4][256]);
+// r <- S_len_i(r) ^ z[i] for i = 0..n-1, len_i = len_each except len_last for the last one
+uint32_t crc32_fold(uint32_t r, const uint32_t* z, size_t n, size_t len_each, size_t len_last);
 
 // Pinned ring of chunk buffers for pipelined copies between a file and
 // device memory: reader/writer threads move chunks between the file (pread /
