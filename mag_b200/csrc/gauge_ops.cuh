@@ -120,12 +120,12 @@ MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, cons
             // D and E are products of links: two rows and a reconstructed third
             const mat3<T> D = mul_nd_su3(U.load_rows01(nu, nb(ci, st, mu, 1)), U.load(mu, nb(ci, st, nu, 1)));
             const mat3<T> E = mul_nd_su3(D, unx);
-            add_to(t, mul_hm(Lam.load(nu, nb(ci, st, mu, 1)), E));
+            mul_hm_acc(t, Lam.load(nu, nb(ci, st, mu, 1)), E);
             herm8<T> dl = Lam.load(nu, st.g);
 #pragma unroll
             for (int k = 0; k < 8; k++) dl.h[k] = lx.h[k] - dl.h[k];
             mat3<T> inner = mul_dn_mh(unx, dl);
-            sub_from(inner, mul_hm_nd(Lam.load(mu, nb(ci, st, nu, 1)), unx));
+            mul_hm_nd_sub(inner, Lam.load(mu, nb(ci, st, nu, 1)), unx);
             mul_acc(t, D, inner);
         }
         {
@@ -138,8 +138,8 @@ MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, cons
 #pragma unroll
             for (int k = 0; k < 8; k++) dl.h[k] -= ln.h[k];
             mat3<T> inner = mul_mh(G, lx);
-            sub_from(inner, mul(mul_dn_mh(umn, dl), unn));
-            sub_from(inner, mul_hm(Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G));
+            mul_sub(inner, mul_dn_mh(umn, dl), unn);
+            mul_hm_sub(inner, Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G);
             mul_dn_acc(t, U.load(nu, nb(ci, st, mu, 1, nu, -1)), inner);
         }
     }
@@ -197,7 +197,7 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
     const cplx<T> t2 = b20 * trW + b21 * trQW + b22 * trQQW;
     // Gamma = t1 Q + t2 Q^2 + f1 W + f2 (Q W + W Q)
     mat3<T> QW = mul_hm(q, W);
-    add_to(QW, mul_mh(W, q));
+    mul_mh_acc(QW, W, q);
     mat3<T> G;
 #pragma unroll
     for (int i = 0; i < 3; i++)

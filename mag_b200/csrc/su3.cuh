@@ -64,179 +64,112 @@ MAG_HD mat3<T> unit_mat() {
     return m;
 }
 
+// ------------------------------------------------------------ products
+// Every product is a chain of fused multiply-adds into one accumulator per
+// real component: c.re <- fma(a.re, b.re, c.re), c.re <- fma(-a.im, b.im, c.re),
+// ...  Written as `c += a.re*b.re - a.im*b.im` the compiler has to form the
+// difference first (a multiply, an fma and an add per real component); the
+// chain below is two fmas per component and term.
+MAG_HD float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+MAG_HD double fmaT(double a, double b, double c) { return fma(a, b, c); }
+
+// s (+/-)= op(a) op(b), op = conjugation when CA / CB; SUB subtracts
+template <bool CA, bool CB, bool SUB, typename T>
+MAG_HD void cmac(cplx<T>& s, cplx<T> a, cplx<T> b) {
+    const T ar = SUB ? -a.re : a.re;
+    const T ai = (SUB != CA) ? -a.im : a.im;  // sign of a.im in op(a), times the sign of the update
+    const T bi = CB ? -b.im : b.im;
+    s.re = fmaT(ar, b.re, s.re);
+    s.re = fmaT(-ai, bi, s.re);
+    s.im = fmaT(ar, bi, s.im);
+    s.im = fmaT(ai, b.re, s.im);
+}
+// s = op(a) op(b)
+template <bool CA, bool CB, typename T>
+MAG_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
+    const T ai = CA ? -a.im : a.im;
+    const T bi = CB ? -b.im : b.im;
+    cplx<T> s;
+    s.re = a.re * b.re;
+    s.re = fmaT(-ai, bi, s.re);
+    s.im = a.re * bi;
+    s.im = fmaT(ai, b.re, s.im);
+    return s;
+}
+
+// rows [0, R) of  c = op(a) op(b)  (ACC = 0),  c += ...  (ACC = 1),  c -= ...  (ACC = -1);
+// TA / TB = 1 take the adjoint of a / b
+template <int R, int TA, int TB, int ACC, typename T>
+MAG_HD void gemm(mat3<T>& c, const mat3<T>& a, const mat3<T>& b) {
+#pragma unroll
+    for (int i = 0; i < R; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<T> s;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const cplx<T> x = TA ? a.e[k][i] : a.e[i][k];
+                const cplx<T> y = TB ? b.e[j][k] : b.e[k][j];
+                if (k == 0 && ACC == 0) s = cmul<TA != 0, TB != 0>(x, y);
+                else {
+                    if (k == 0) s = c.e[i][j];
+                    cmac<TA != 0, TB != 0, (ACC < 0)>(s, x, y);
+                }
+            }
+            c.e[i][j] = s;
+        }
+}
+
 // c = a * b
 template <typename T>
-MAG_HD mat3<T> mul(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[i][0].re * b.e[0][j].re - a.e[i][0].im * b.e[0][j].im;
-            T im = a.e[i][0].re * b.e[0][j].im + a.e[i][0].im * b.e[0][j].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[i][k].re * b.e[k][j].re - a.e[i][k].im * b.e[k][j].im;
-                im += a.e[i][k].re * b.e[k][j].im + a.e[i][k].im * b.e[k][j].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
+MAG_HD mat3<T> mul(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<3, 0, 0, 0>(c, a, b); return c; }
 // c = a * b^dag
 template <typename T>
-MAG_HD mat3<T> mul_nd(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[i][0].re * b.e[j][0].re + a.e[i][0].im * b.e[j][0].im;
-            T im = -a.e[i][0].re * b.e[j][0].im + a.e[i][0].im * b.e[j][0].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[i][k].re * b.e[j][k].re + a.e[i][k].im * b.e[j][k].im;
-                im += -a.e[i][k].re * b.e[j][k].im + a.e[i][k].im * b.e[j][k].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
+MAG_HD mat3<T> mul_nd(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<3, 0, 1, 0>(c, a, b); return c; }
 // c = a^dag * b
 template <typename T>
-MAG_HD mat3<T> mul_dn(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[0][i].re * b.e[0][j].re + a.e[0][i].im * b.e[0][j].im;
-            T im = a.e[0][i].re * b.e[0][j].im - a.e[0][i].im * b.e[0][j].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[k][i].re * b.e[k][j].re + a.e[k][i].im * b.e[k][j].im;
-                im += a.e[k][i].re * b.e[k][j].im - a.e[k][i].im * b.e[k][j].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
-// acc += a * b
+MAG_HD mat3<T> mul_dn(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<3, 1, 0, 0>(c, a, b); return c; }
+// acc += a * b, a * b^dag, a^dag * b
 template <typename T>
-MAG_HD void mul_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = acc.e[i][j].re, im = acc.e[i][j].im;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                re += a.e[i][k].re * b.e[k][j].re - a.e[i][k].im * b.e[k][j].im;
-                im += a.e[i][k].re * b.e[k][j].im + a.e[i][k].im * b.e[k][j].re;
-            }
-            acc.e[i][j] = mk(re, im);
-        }
-}
-// acc += a * b^dag
+MAG_HD void mul_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 0, 0, 1>(acc, a, b); }
 template <typename T>
-MAG_HD void mul_nd_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = acc.e[i][j].re, im = acc.e[i][j].im;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                re += a.e[i][k].re * b.e[j][k].re + a.e[i][k].im * b.e[j][k].im;
-                im += -a.e[i][k].re * b.e[j][k].im + a.e[i][k].im * b.e[j][k].re;
-            }
-            acc.e[i][j] = mk(re, im);
-        }
-}
-// acc += a^dag * b
+MAG_HD void mul_nd_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 0, 1, 1>(acc, a, b); }
 template <typename T>
-MAG_HD void mul_dn_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) {
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = acc.e[i][j].re, im = acc.e[i][j].im;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                re += a.e[k][i].re * b.e[k][j].re + a.e[k][i].im * b.e[k][j].im;
-                im += a.e[k][i].re * b.e[k][j].im - a.e[k][i].im * b.e[k][j].re;
-            }
-            acc.e[i][j] = mk(re, im);
-        }
-}
+MAG_HD void mul_dn_acc(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 1, 0, 1>(acc, a, b); }
+// acc -= a * b
+template <typename T>
+MAG_HD void mul_sub(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 0, 0, -1>(acc, a, b); }
 
 // ------------------------------------------------ special-unitary products
 // A product of SU(3) matrices is in SU(3), so its third row is conj(row0 x
 // row1): two rows cost 18 complex multiply-adds instead of 27, and only rows
 // 0, 1 of the left factor are read.
 template <typename T>
+MAG_HD cplx<T> cross_conj(cplx<T> a, cplx<T> b, cplx<T> c, cplx<T> d) {  // conj(a b - c d)
+    cplx<T> s;
+    s.re = a.re * b.re;
+    s.re = fmaT(-a.im, b.im, s.re);
+    s.re = fmaT(-c.re, d.re, s.re);
+    s.re = fmaT(c.im, d.im, s.re);
+    s.im = c.re * d.im;
+    s.im = fmaT(c.im, d.re, s.im);
+    s.im = fmaT(-a.re, b.im, s.im);
+    s.im = fmaT(-a.im, b.re, s.im);
+    return s;
+}
+template <typename T>
 MAG_HD void reconstruct_row2(mat3<T>& m) {
-    m.e[2][0] = conj(m.e[0][1] * m.e[1][2] - m.e[0][2] * m.e[1][1]);
-    m.e[2][1] = conj(m.e[0][2] * m.e[1][0] - m.e[0][0] * m.e[1][2]);
-    m.e[2][2] = conj(m.e[0][0] * m.e[1][1] - m.e[0][1] * m.e[1][0]);
+    m.e[2][0] = cross_conj(m.e[0][1], m.e[1][2], m.e[0][2], m.e[1][1]);
+    m.e[2][1] = cross_conj(m.e[0][2], m.e[1][0], m.e[0][0], m.e[1][2]);
+    m.e[2][2] = cross_conj(m.e[0][0], m.e[1][1], m.e[0][1], m.e[1][0]);
 }
-// rows 0, 1 of a * b (row 2 of the result left unset)
+// rows 0, 1 of a * b, a * b^dag, a^dag * b (row 2 of the result left unset)
 template <typename T>
-MAG_HD mat3<T> mul_2r(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[i][0].re * b.e[0][j].re - a.e[i][0].im * b.e[0][j].im;
-            T im = a.e[i][0].re * b.e[0][j].im + a.e[i][0].im * b.e[0][j].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[i][k].re * b.e[k][j].re - a.e[i][k].im * b.e[k][j].im;
-                im += a.e[i][k].re * b.e[k][j].im + a.e[i][k].im * b.e[k][j].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
-// rows 0, 1 of a * b^dag
+MAG_HD mat3<T> mul_2r(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<2, 0, 0, 0>(c, a, b); return c; }
 template <typename T>
-MAG_HD mat3<T> mul_nd_2r(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[i][0].re * b.e[j][0].re + a.e[i][0].im * b.e[j][0].im;
-            T im = -a.e[i][0].re * b.e[j][0].im + a.e[i][0].im * b.e[j][0].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[i][k].re * b.e[j][k].re + a.e[i][k].im * b.e[j][k].im;
-                im += -a.e[i][k].re * b.e[j][k].im + a.e[i][k].im * b.e[j][k].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
-// rows 0, 1 of a^dag * b
+MAG_HD mat3<T> mul_nd_2r(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<2, 0, 1, 0>(c, a, b); return c; }
 template <typename T>
-MAG_HD mat3<T> mul_dn_2r(const mat3<T>& a, const mat3<T>& b) {
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            T re = a.e[0][i].re * b.e[0][j].re + a.e[0][i].im * b.e[0][j].im;
-            T im = a.e[0][i].re * b.e[0][j].im - a.e[0][i].im * b.e[0][j].re;
-#pragma unroll
-            for (int k = 1; k < 3; k++) {
-                re += a.e[k][i].re * b.e[k][j].re + a.e[k][i].im * b.e[k][j].im;
-                im += a.e[k][i].re * b.e[k][j].im - a.e[k][i].im * b.e[k][j].re;
-            }
-            c.e[i][j] = mk(re, im);
-        }
-    return c;
-}
+MAG_HD mat3<T> mul_dn_2r(const mat3<T>& a, const mat3<T>& b) { mat3<T> c; gemm<2, 1, 0, 0>(c, a, b); return c; }
 // full SU(3) products through two rows + reconstruction
 template <typename T>
 MAG_HD mat3<T> mul_su3(const mat3<T>& a, const mat3<T>& b) {
@@ -297,7 +230,7 @@ MAG_HD void caxpy(mat3<T>& a, cplx<T> z, const mat3<T>& b) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) a.e[i][j] = a.e[i][j] + z * b.e[i][j];
+        for (int j = 0; j < 3; j++) cmac<false, false, false>(a.e[i][j], z, b.e[i][j]);
 }
 template <typename T>
 MAG_HD mat3<T> scaled(const mat3<T>& a, T s) {
@@ -327,7 +260,10 @@ MAG_HD T retr_mul(const mat3<T>& a, const mat3<T>& b) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int k = 0; k < 3; k++) s += a.e[i][k].re * b.e[k][i].re - a.e[i][k].im * b.e[k][i].im;
+        for (int k = 0; k < 3; k++) {
+            s = fmaT(a.e[i][k].re, b.e[k][i].re, s);
+            s = fmaT(-a.e[i][k].im, b.e[k][i].im, s);
+        }
     return s;
 }
 // Tr(a * b)
@@ -337,7 +273,7 @@ MAG_HD cplx<T> tr_mul(const mat3<T>& a, const mat3<T>& b) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int k = 0; k < 3; k++) s = s + a.e[i][k] * b.e[k][i];
+        for (int k = 0; k < 3; k++) cmac<false, false, false>(s, a.e[i][k], b.e[k][i]);
     return s;
 }
 template <typename T, typename S>
@@ -396,80 +332,58 @@ MAG_HD void herm_rows(const herm8<T>& q, cplx<T> H[3][3]) {
     H[1][2] = mk<T>(q.h[6], q.h[7]);
     H[2][1] = mk<T>(q.h[6], -q.h[7]);
 }
-template <typename T>
-MAG_HD cplx<T> rmul(T r, cplx<T> z) { return mk(r * z.re, r * z.im); }
-// H X
-template <typename T>
-MAG_HD mat3<T> mul_hm(const herm8<T>& q, const mat3<T>& x) {
+// c (=, +=, -=) H op(X)  (SIDE = 0)  or  op(X) H  (SIDE = 1); TX = 1: op(X) = X^dag
+template <int SIDE, int TX, int ACC, typename T>
+MAG_HD void hgemm(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) {
     cplx<T> H[3][3];
     herm_rows(q, H);
-    mat3<T> c;
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            cplx<T> s = rmul(H[i][i].re, x.e[i][j]);
+            const int d = SIDE == 0 ? i : j;  // index of the real diagonal element of H in this sum
+            cplx<T> s;
+            if (ACC == 0) {
+                const cplx<T> xd = TX ? conj(SIDE == 0 ? x.e[j][d] : x.e[d][i]) : (SIDE == 0 ? x.e[d][j] : x.e[i][d]);
+                s = mk(H[d][d].re * xd.re, H[d][d].re * xd.im);
+            } else {
+                s = c.e[i][j];
+                const cplx<T> xd = TX ? conj(SIDE == 0 ? x.e[j][d] : x.e[d][i]) : (SIDE == 0 ? x.e[d][j] : x.e[i][d]);
+                const T h = ACC < 0 ? -H[d][d].re : H[d][d].re;
+                s.re = fmaT(h, xd.re, s.re);
+                s.im = fmaT(h, xd.im, s.im);
+            }
 #pragma unroll
-            for (int k = 0; k < 3; k++)
-                if (k != i) s = s + H[i][k] * x.e[k][j];
+            for (int k = 0; k < 3; k++) {
+                if (k == d) continue;
+                if (SIDE == 0) {  // H[i][k] op(X)[k][j]
+                    const cplx<T> xk = TX ? x.e[j][k] : x.e[k][j];
+                    cmac<false, TX != 0, (ACC < 0)>(s, H[i][k], xk);
+                } else {          // op(X)[i][k] H[k][j]
+                    const cplx<T> xk = TX ? x.e[k][i] : x.e[i][k];
+                    cmac<TX != 0, false, (ACC < 0)>(s, xk, H[k][j]);
+                }
+            }
             c.e[i][j] = s;
         }
-    return c;
 }
-// H X^dag
+// H X, H X^dag, X H, X^dag H and their accumulating forms
 template <typename T>
-MAG_HD mat3<T> mul_hm_nd(const herm8<T>& q, const mat3<T>& x) {
-    cplx<T> H[3][3];
-    herm_rows(q, H);
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            cplx<T> s = rmul(H[i][i].re, conj(x.e[j][i]));
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-                if (k != i) s = s + H[i][k] * conj(x.e[j][k]);
-            c.e[i][j] = s;
-        }
-    return c;
-}
-// X H
+MAG_HD mat3<T> mul_hm(const herm8<T>& q, const mat3<T>& x) { mat3<T> c; hgemm<0, 0, 0>(c, q, x); return c; }
 template <typename T>
-MAG_HD mat3<T> mul_mh(const mat3<T>& x, const herm8<T>& q) {
-    cplx<T> H[3][3];
-    herm_rows(q, H);
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            cplx<T> s = rmul(H[j][j].re, x.e[i][j]);
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-                if (k != j) s = s + x.e[i][k] * H[k][j];
-            c.e[i][j] = s;
-        }
-    return c;
-}
-// X^dag H
+MAG_HD mat3<T> mul_hm_nd(const herm8<T>& q, const mat3<T>& x) { mat3<T> c; hgemm<0, 1, 0>(c, q, x); return c; }
 template <typename T>
-MAG_HD mat3<T> mul_dn_mh(const mat3<T>& x, const herm8<T>& q) {
-    cplx<T> H[3][3];
-    herm_rows(q, H);
-    mat3<T> c;
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            cplx<T> s = rmul(H[j][j].re, conj(x.e[j][i]));
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-                if (k != j) s = s + conj(x.e[k][i]) * H[k][j];
-            c.e[i][j] = s;
-        }
-    return c;
-}
+MAG_HD mat3<T> mul_mh(const mat3<T>& x, const herm8<T>& q) { mat3<T> c; hgemm<1, 0, 0>(c, q, x); return c; }
+template <typename T>
+MAG_HD mat3<T> mul_dn_mh(const mat3<T>& x, const herm8<T>& q) { mat3<T> c; hgemm<1, 1, 0>(c, q, x); return c; }
+template <typename T>
+MAG_HD void mul_hm_acc(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) { hgemm<0, 0, 1>(c, q, x); }
+template <typename T>
+MAG_HD void mul_hm_sub(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) { hgemm<0, 0, -1>(c, q, x); }
+template <typename T>
+MAG_HD void mul_hm_nd_sub(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) { hgemm<0, 1, -1>(c, q, x); }
+template <typename T>
+MAG_HD void mul_mh_acc(mat3<T>& c, const mat3<T>& x, const herm8<T>& q) { hgemm<1, 0, 1>(c, q, x); }
 
 // F = i s TA(M),  TA(M) = 1/2 (M - M^dag) - 1/6 Tr(M - M^dag)  (cps TrLessAntiHermMatrix)
 template <typename T>
