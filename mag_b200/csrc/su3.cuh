@@ -464,6 +464,15 @@ struct ch_coef {
 };
 
 // c0 = Re Tr(Q^3)/3, c1 = Re Tr(Q^2)/2 as supplied by the caller.
+MAG_HD void sincos_hd(double x, double& s, double& c) {
+#if defined(__CUDA_ARCH__)
+    sincos(x, &s, &c);
+#else
+    s = sin(x);
+    c = cos(x);
+#endif
+}
+
 template <bool WITH_B>
 MAG_HD ch_coef ch_coefficients(double c0, double c1) {
     ch_coef r;
@@ -477,25 +486,34 @@ MAG_HD ch_coef ch_coefficients(double c0, double c1) {
         r.b20r = r.b20i = r.b21r = r.b21i = r.b22r = r.b22i = 0.0;
         return r;
     }
-    const double c0m = 2.0 * pow(c1 / 3.0, 1.5);
+    // The same quantities as the reference (field-hmc.h:90-110), evaluated with
+    // fewer library calls: (c1/3)^1.5 = t sqrt(t), sqrt(c1) = sqrt(3) sqrt(c1/3),
+    // sine and cosine of one argument from one sincos, cos 2u and sin 2u by the
+    // double-angle formulas, divisions by den as products with 1/den.
+    const double t3 = c1 / 3.0, st3 = sqrt(t3);
+    const double c0m = 2.0 * t3 * st3;
     double ratio = c0 / c0m;
     if (ratio > 1.0) ratio = 1.0;  // rounding guard (reference would return NaN)
     const double theta = acos(ratio);
-    const double u = sqrt(c1 / 3.0) * cos(theta / 3.0);
-    const double w = sqrt(c1) * sin(theta / 3.0);
+    double sth, cth;
+    sincos_hd(theta / 3.0, sth, cth);
+    const double u = st3 * cth;
+    const double w = 1.7320508075688772 * st3 * sth;  // sqrt(c1) sin(theta / 3)
     const double ww = w * w, uu = u * u;
+    double sw, cw;
+    sincos_hd(w, sw, cw);
     double xi0, xi1 = 0.0;
     if (ww < 0.05 * 0.05) {
         xi0 = 1. - ww / 6. * (1. - ww / 20. * (1. - ww / 42.));
         if (WITH_B) xi1 = -1. / 2. * (1. - ww / 12. * (1. - ww / 30.)) + 1. / 6. * (1. - ww / 20. * (1. - ww / 42.));
     } else {
-        const double sw = sin(w);
-        xi0 = sw / w;
-        if (WITH_B) xi1 = cos(w) / ww - sw / (ww * w);
+        const double iw = 1.0 / w;
+        xi0 = sw * iw;
+        if (WITH_B) xi1 = (cw - xi0) * iw * iw;  // cos(w)/w^2 - sin(w)/w^3
     }
-    const double cw = cos(w);
-    const double c2u = cos(2. * u), s2u = sin(2. * u);
-    const double cu = cos(u), su = sin(u);
+    double su, cu;
+    sincos_hd(u, su, cu);
+    const double c2u = (cu - su) * (cu + su), s2u = 2.0 * su * cu;
     // e2u = exp(2iu), emu = exp(-iu)
     // h0 = (u^2-w^2) e2u + emu (8u^2 cos w + i 2u(3u^2+w^2) xi0)
     const double a0r = 8. * uu * cw, a0i = 2. * u * (3. * uu + ww) * xi0;
@@ -509,8 +527,9 @@ MAG_HD ch_coef ch_coefficients(double c0, double c1) {
     const double a2r = cw, a2i = 3. * u * xi0;
     const double h2r = c2u - (cu * a2r + su * a2i);
     const double h2i = s2u - (cu * a2i - su * a2r);
-    const double den = 9. * uu - ww;
-    double f0r = h0r / den, f0i = h0i / den, f1r = h1r / den, f1i = h1i / den, f2r = h2r / den, f2i = h2i / den;
+    const double den = 9. * uu - ww, iden = 1.0 / den;
+    double f0r = h0r * iden, f0i = h0i * iden, f1r = h1r * iden, f1i = h1i * iden, f2r = h2r * iden,
+           f2i = h2i * iden;
     if (WITH_B) {
         // complex helpers in (re, im) pairs
         // r01 = 2(u + i(u^2-w^2)) e2u + 2 emu (4u(2 - iu) cos w + i xi0 (9u^2 + w^2 - iu(3u^2+w^2)))
@@ -543,20 +562,20 @@ MAG_HD ch_coef ch_coefficients(double c0, double c1) {
         // r22 = emu (xi0 - 3iu xi1)
         const double Hr = xi0, Hi = -3. * u * xi1;
         const double r22r = cu * Hr + su * Hi, r22i = cu * Hi - su * Hr;
-        const double bden = 2. * den * den;
+        const double ibden = 0.5 * iden * iden;  // 1 / (2 den^2)
         const double k1 = 3. * uu - ww, k2 = 2. * (15. * uu + ww);
-        r.b10r = (2. * u * r01r + k1 * r02r - k2 * f0r) / bden;
-        r.b10i = (2. * u * r01i + k1 * r02i - k2 * f0i) / bden;
-        r.b11r = (2. * u * r11r + k1 * r12r - k2 * f1r) / bden;
-        r.b11i = (2. * u * r11i + k1 * r12i - k2 * f1i) / bden;
-        r.b12r = (2. * u * r21r + k1 * r22r - k2 * f2r) / bden;
-        r.b12i = (2. * u * r21i + k1 * r22i - k2 * f2i) / bden;
-        r.b20r = (r01r - 3. * u * r02r - 24. * u * f0r) / bden;
-        r.b20i = (r01i - 3. * u * r02i - 24. * u * f0i) / bden;
-        r.b21r = (r11r - 3. * u * r12r - 24. * u * f1r) / bden;
-        r.b21i = (r11i - 3. * u * r12i - 24. * u * f1i) / bden;
-        r.b22r = (r21r - 3. * u * r22r - 24. * u * f2r) / bden;
-        r.b22i = (r21i - 3. * u * r22i - 24. * u * f2i) / bden;
+        r.b10r = (2. * u * r01r + k1 * r02r - k2 * f0r) * ibden;
+        r.b10i = (2. * u * r01i + k1 * r02i - k2 * f0i) * ibden;
+        r.b11r = (2. * u * r11r + k1 * r12r - k2 * f1r) * ibden;
+        r.b11i = (2. * u * r11i + k1 * r12i - k2 * f1i) * ibden;
+        r.b12r = (2. * u * r21r + k1 * r22r - k2 * f2r) * ibden;
+        r.b12i = (2. * u * r21i + k1 * r22i - k2 * f2i) * ibden;
+        r.b20r = (r01r - 3. * u * r02r - 24. * u * f0r) * ibden;
+        r.b20i = (r01i - 3. * u * r02i - 24. * u * f0i) * ibden;
+        r.b21r = (r11r - 3. * u * r12r - 24. * u * f1r) * ibden;
+        r.b21i = (r11i - 3. * u * r12i - 24. * u * f1i) * ibden;
+        r.b22r = (r21r - 3. * u * r22r - 24. * u * f2r) * ibden;
+        r.b22i = (r21i - 3. * u * r22i - 24. * u * f2i) * ibden;
         if (reflect) {
             r.b10i = -r.b10i;                 // conj
             r.b11r = -r.b11r;                 // -conj
