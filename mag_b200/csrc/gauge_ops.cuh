@@ -153,16 +153,22 @@ template <typename T>
 MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul, herm8<T>& lam, mat3<T>& zp) {
     const mat3<T> Q = expand(q);
     const mat3<T> QQ = mul_hm(q, Q);
-    ch_coef_f cf;
-    ch_coef c;
+    cplx<T> f0, f1, f2, b10, b11, b12, b20, b21, b22;
     bool nontrivial;
     if constexpr (sizeof(T) == 4) {
-        nontrivial = ch_for<T, true>(Q, QQ, cf);  // FP32: power series (see su3.cuh)
+        ch_coef_f c;
+        nontrivial = ch_for<T, true>(Q, QQ, c);  // FP32: power series (see su3.cuh)
+        f0 = mk(c.f0r, c.f0i); f1 = mk(c.f1r, c.f1i); f2 = mk(c.f2r, c.f2i);
+        b10 = mk(c.b10r, c.b10i); b11 = mk(c.b11r, c.b11i); b12 = mk(c.b12r, c.b12i);
+        b20 = mk(c.b20r, c.b20i); b21 = mk(c.b21r, c.b21i); b22 = mk(c.b22r, c.b22i);
     } else {
         double c0, c1;
         ch_invariants(Q, QQ, c0, c1);
-        c = ch_coefficients<true>(c0, c1);  // FP64: the reference's closed form
+        const ch_coef c = ch_coefficients<true>(c0, c1);  // FP64: the reference's closed form
         nontrivial = !c.trivial;
+        f0 = mk<T>(c.f0r, c.f0i); f1 = mk<T>(c.f1r, c.f1i); f2 = mk<T>(c.f2r, c.f2i);
+        b10 = mk<T>(c.b10r, c.b10i); b11 = mk<T>(c.b11r, c.b11i); b12 = mk<T>(c.b12r, c.b12i);
+        b20 = mk<T>(c.b20r, c.b20i); b21 = mk<T>(c.b21r, c.b21i); b22 = mk<T>(c.b22r, c.b22i);
     }
     if (!nontrivial) {
         // c1 = 0: exp(iQ) = 1 and Lambda = 0 (field-multi.h:190)
@@ -170,31 +176,29 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
         lam = herm_zero<T>();
         return;
     }
-    if constexpr (sizeof(T) == 4) {
-        c.f0r = cf.f0r; c.f0i = cf.f0i; c.f1r = cf.f1r; c.f1i = cf.f1i; c.f2r = cf.f2r; c.f2i = cf.f2i;
-        c.b10r = cf.b10r; c.b10i = cf.b10i; c.b11r = cf.b11r; c.b11i = cf.b11i; c.b12r = cf.b12r; c.b12i = cf.b12i;
-        c.b20r = cf.b20r; c.b20i = cf.b20i; c.b21r = cf.b21r; c.b21i = cf.b21i; c.b22r = cf.b22r; c.b22i = cf.b22i;
-    }
-    const cplx<T> f0 = mk<T>((T)c.f0r, (T)c.f0i), f1 = mk<T>((T)c.f1r, (T)c.f1i), f2 = mk<T>((T)c.f2r, (T)c.f2i);
-    // exp(iQ) and Z' exp(iQ)
+    // exp(iQ) = f0 + f1 Q + f2 Q^2 and Z' exp(iQ)
     mat3<T> eq;
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) eq.e[i][j] = f1 * Q.e[i][j] + f2 * QQ.e[i][j];
+        for (int j = 0; j < 3; j++) {
+            cplx<T> e = cmul<false, false>(f1, Q.e[i][j]);
+            cmac<false, false, false>(e, f2, QQ.e[i][j]);
+            eq.e[i][j] = e;
+        }
 #pragma unroll
     for (int i = 0; i < 3; i++) eq.e[i][i] = eq.e[i][i] + f0;
     zp = mul(Z, eq);
     const mat3<T> W = mul(Ul, Z);  // U Sigma'
-    const cplx<T> b10 = mk<T>((T)c.b10r, (T)c.b10i), b11 = mk<T>((T)c.b11r, (T)c.b11i),
-                  b12 = mk<T>((T)c.b12r, (T)c.b12i);
-    const cplx<T> b20 = mk<T>((T)c.b20r, (T)c.b20i), b21 = mk<T>((T)c.b21r, (T)c.b21i),
-                  b22 = mk<T>((T)c.b22r, (T)c.b22i);
     // Tr(Sigma' B U) = Tr(B W) with B = b0 + b1 Q + b2 Q^2
     const cplx<T> trW = mk<T>(W.e[0][0].re + W.e[1][1].re + W.e[2][2].re, W.e[0][0].im + W.e[1][1].im + W.e[2][2].im);
     const cplx<T> trQW = tr_mul(Q, W), trQQW = tr_mul(QQ, W);
-    const cplx<T> t1 = b10 * trW + b11 * trQW + b12 * trQQW;
-    const cplx<T> t2 = b20 * trW + b21 * trQW + b22 * trQQW;
+    cplx<T> t1 = cmul<false, false>(b10, trW);
+    cmac<false, false, false>(t1, b11, trQW);
+    cmac<false, false, false>(t1, b12, trQQW);
+    cplx<T> t2 = cmul<false, false>(b20, trW);
+    cmac<false, false, false>(t2, b21, trQW);
+    cmac<false, false, false>(t2, b22, trQQW);
     // Gamma = t1 Q + t2 Q^2 + f1 W + f2 (Q W + W Q)
     mat3<T> QW = mul_hm(q, W);
     mul_mh_acc(QW, W, q);
@@ -202,7 +206,13 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) G.e[i][j] = t1 * Q.e[i][j] + t2 * QQ.e[i][j] + f1 * W.e[i][j] + f2 * QW.e[i][j];
+        for (int j = 0; j < 3; j++) {
+            cplx<T> g = cmul<false, false>(t1, Q.e[i][j]);
+            cmac<false, false, false>(g, t2, QQ.e[i][j]);
+            cmac<false, false, false>(g, f1, W.e[i][j]);
+            cmac<false, false, false>(g, f2, QW.e[i][j]);
+            G.e[i][j] = g;
+        }
     lam = herm_traceless(G);
 }
 

@@ -624,9 +624,10 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
     float B1[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
     float B2[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
     float coef = 1.f;    // 1/n!
-    float bound = 1.f;   // max(q, 1)^n / n!: the a_n, b_n, d_n and their derivatives
-                         // carry powers of q down to q^(n-5), so q < 1 counts as 1
-    const float q = fmaxf(sqrtf(q2), 1.f);
+    float bound = 1.f;   // q^n / n! for q >= 1, q^(n-5) / n! for q < 1: the a_n, b_n, d_n
+                         // and their derivatives carry powers of q down to q^(n-5)
+    const float q = sqrtf(q2);
+    const bool qbig = q >= 1.f;
 #pragma unroll 1
     for (int n = 1; n < 40; n++) {
         // advance Q^{n-1} -> Q^n (and the derivatives)
@@ -639,7 +640,7 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
         }
         a = na; b = nb; d = nd;
         coef /= (float)n;
-        bound *= q / (float)n;
+        bound *= (qbig || n > 5 ? q : 1.f) / (float)n;
         // i^n/n!: real for even n (sign (-1)^{n/2}), imaginary for odd n
         const int part = n & 1;
         const float s = ((n >> 1) & 1) ? -coef : coef;
@@ -748,7 +749,11 @@ MAG_HD mat3<T> expiQ(const herm8<T>& q) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
-        for (int j = 0; j < 3; j++) r.e[i][j] = f1 * Q.e[i][j] + f2 * QQ.e[i][j];
+        for (int j = 0; j < 3; j++) {
+            cplx<T> e = cmul<false, false>(f1, Q.e[i][j]);
+            cmac<false, false, false>(e, f2, QQ.e[i][j]);
+            r.e[i][j] = e;
+        }
 #pragma unroll
     for (int i = 0; i < 3; i++) r.e[i][i] = r.e[i][i] + f0;
     return r;
