@@ -287,10 +287,11 @@ def reference_arm(args, params, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
-def config_of(name, params, world):
+def config_of(name, params, world, shard=False):
     c = {"workload": name, "action": "iwasaki", "c1": params["c1"], "stout_levels": params["n_stout"],
          "rho": params["rho"], "fg_steps": params["n_steps"], "tau": params["tau"], "mag": params["mag"],
-         "precision": params["precision"], "accept": "metropolis", "parallelism": f"replicas{world}",
+         "precision": params["precision"], "accept": "metropolis",
+         "parallelism": f"chains split over {world} GPUs" if shard else f"replicas{world}",
          "l2": "working set > 126 MB L2 (links, momenta, stout levels)"}
     if "chains" in params:
         c["chains"] = "48x8^4 + 32x12^4 + 16x16^4, beta ~ U[2.0, 2.6) per chain"
@@ -320,14 +321,29 @@ def run_gpu(args, params, rank, world, dist):
     import mag_b200 as M
     from mag_b200.field_hmc import probe_fma_peak
 
-    V = total_sites(params)
     n = params["n_steps"]
+    full_params = params
+    # an ensemble on N > 1 GPUs is split over the ranks (balanced by V x steps), each chain
+    # keeping its Philox stream; a single lattice runs as N independent replicas
+    shard = "chains" in params and world > 1
+    parts = None
+    if shard:
+        from mag_b200.ensemble import chain_cost, partition
+
+        parts = partition([chain_cost(ch["dims"], n) for ch in params["chains"]], world)
+        params = dict(params)
+        params["chains"] = [full_params["chains"][i] for i in parts[rank]]
+    V = total_sites(params)
     nchain = len(params["chains"]) if "chains" in params else 1
-    seed = rank_seed(rank)
+    job_chains = len(full_params["chains"]) if shard else world * nchain  # chains advanced per step, all ranks
+    job_sites = total_sites(full_params) if shard else world * V
+    seed = rank_seed(0) if shard else rank_seed(rank)
     wl = params.get("wilson", 0)
 
     def timed_run(prec: str):
         c = make_ctx(M, params, seed, prec, args.warmup)
+        if shard:
+            c.set_stream_index(parts[rank])
         c.hot_start(seed)
         if args.warmup:
             c.run_chmc(args.warmup)
@@ -356,10 +372,15 @@ def run_gpu(args, params, rank, world, dist):
 
     head_prec = params["precision"]
     c64, rec64, ms64, wl_ms, clocks = timed_run(head_prec)
-    value = world * nchain * args.steps / (ms64 / 1e3)
+    value = job_chains * args.steps / (ms64 / 1e3)
     ms_per_step = ms64 / args.steps
-    dh = [r[k]["delta_h"] for r in rec64 for k in range(nchain)]
-    acc = [r[k]["accept"] for r in rec64 for k in range(nchain)]
+    if shard:
+        from mag_b200.ensemble import gather_records
+
+        rec64 = gather_records(rec64, parts, rank, dist, "cuda")  # every rank, same shapes
+    nrec = len(rec64[0])
+    dh = [r[k]["delta_h"] for r in rec64 for k in range(nrec)]
+    acc = [r[k]["accept"] for r in rec64 for k in range(nrec)]
     plaq = rec64[-1][0]["avg_plaquette"]
     kernels_per_traj = c64.graph_kernel_count()
 
@@ -445,7 +466,7 @@ def run_gpu(args, params, rank, world, dist):
     mixed = None
     if not args.no_mixed and head_prec == "fp64":
         cm, recm, msm, _, _ = timed_run("mixed")
-        vm = world * nchain * args.steps / (msm / 1e3)
+        vm = job_chains * args.steps / (msm / 1e3)
         mixed = {"value": vm, "unit": "traj/s", "ms_per_step": msm / args.steps, "speedup_vs_fp64": vm / value,
                  "delta_h_mean": statistics.fmean(r[0]["delta_h"] for r in recm),
                  "acceptance": statistics.fmean(r[0]["accept"] for r in recm),
@@ -469,12 +490,13 @@ def run_gpu(args, params, rank, world, dist):
         return
     line = {
         "metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "strong" if shard else "weak",
         "vs_baseline": None, "dtype": "f64" if head_prec == "fp64" else "f32+f64",
         "data": "synthetic: Philox Haar-random hot start, Gaussian momenta, Philox Metropolis uniforms",
-        "config": config_of(args.workload, params, world),
-        "force_evals_per_s": world * nchain * 4 * n * args.steps / (ms64 / 1e3),
-        "site_updates_per_s": world * V * 4 * n * args.steps / (ms64 / 1e3),
+        "config": config_of(args.workload, full_params, world, shard),
+        "force_evals_per_s": job_chains * 4 * n * args.steps / (ms64 / 1e3),
+        "site_updates_per_s": job_sites * 4 * n * args.steps / (ms64 / 1e3),
         "delta_h_mean": statistics.fmean(dh), "delta_h_abs_mean": statistics.fmean(abs(x) for x in dh),
         "acceptance": statistics.fmean(acc), "plaquette": plaq,
         "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,

@@ -123,12 +123,22 @@ int mag_kinetic(mag_ctx* ctx, int chain, double* kinetic);
 int mag_hamiltonian(mag_ctx* ctx, int chain, double out[3]);
 /* evolve_gauge_field (field-hmc.h:442-482): U <- exp(i eps P) U with the constraint rules */
 int mag_evolve_gauge(mag_ctx* ctx, double eps);
+/* evolve_gauge_field driven by the momenta (MAG_SRC_MOMENTA, as mag_evolve_gauge) or by the
+   force of the current links (MAG_SRC_FORCE: U <- exp(i eps F(U)) U, the force-gradient
+   step's link update, field-hmc.h:497-503) */
+enum { MAG_SRC_MOMENTA = 0, MAG_SRC_FORCE = 1 };
+int mag_evolve_gauge_src(mag_ctx* ctx, double eps, int src);
 /* evolve_momentum (field-hmc.h:427-440) with the force of the current links: P += eps F(U) */
 int mag_evolve_momentum(mag_ctx* ctx, double eps);
 /* reunitarize (field-matrix.h:83-100); maxdev[chain] = max |U' - U| */
 int mag_reunitarize(mag_ctx* ctx, double* maxdev);
 /* stout smearing forward of one chain: level k of the smeared links (k = 0 thin) */
 int mag_stout_level(mag_ctx* ctx, int chain, int level, double* host_aos);
+/* the same under the name of the stout entry points: mag_stout_forward = mag_stout_level;
+   mag_stout_force = the force through the stout chain rule (mag_gauge_force of a context
+   with n_stout >= 1; MAG_ERR_STATE without stout levels) */
+int mag_stout_forward(mag_ctx* ctx, int chain, int level, double* host_aos);
+int mag_stout_force(mag_ctx* ctx, int chain, double* host_force_aos);
 
 /* ------------------------------------------------------------ integrator */
 /* force_gradient_integrator (field-hmc.h:525-567) or leap_frog_integrator
@@ -143,6 +153,17 @@ int mag_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results);
 /* n trajectories back to back with Philox momenta, the whole trajectory
    replayed as one CUDA graph; results[n * n_chains] in trajectory-major order */
 int mag_run(mag_ctx* ctx, int n_traj, mag_traj_result* results);
+/* the trajectory and ensemble entry points under their batch names:
+   mag_fg_trajectory = mag_trajectory, mag_batch_create = mag_ensemble_create,
+   mag_batch_run = mag_run */
+int mag_fg_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results);
+int mag_batch_create(const mag_params* p, int n_chains, mag_ctx** out);
+int mag_batch_run(mag_ctx* ctx, int n_traj, mag_traj_result* results);
+/* Philox stream of each chain: chain c's key is seed + index[c] for the hot start,
+   the momenta and the Metropolis uniforms (default index[c] = c).  A job that splits
+   one ensemble over several contexts (one per GPU) passes each chain's position in the
+   whole ensemble, so every chain draws the numbers it would draw in one context. */
+int mag_set_stream_index(mag_ctx* ctx, const int64_t* index);
 /* number of trajectories done so far (the Philox trajectory counter) */
 int mag_traj_counter(mag_ctx* ctx, int64_t* traj);
 int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);

@@ -123,6 +123,13 @@ SIGNATURES = {
     "mag_hamiltonian": [_CTX, ctypes.c_int, _DP],
     "mag_evolve_gauge": [_CTX, ctypes.c_double],
     "mag_evolve_momentum": [_CTX, ctypes.c_double],
+    "mag_evolve_gauge_src": [_CTX, ctypes.c_double, ctypes.c_int],
+    "mag_stout_forward": [_CTX, ctypes.c_int, ctypes.c_int, _DP],
+    "mag_stout_force": [_CTX, ctypes.c_int, _DP],
+    "mag_fg_trajectory": [_CTX, ctypes.c_int, ctypes.POINTER(TrajResult)],
+    "mag_batch_create": [ctypes.POINTER(MagParams), ctypes.c_int, ctypes.POINTER(_CTX)],
+    "mag_batch_run": [_CTX, ctypes.c_int, ctypes.POINTER(TrajResult)],
+    "mag_set_stream_index": [_CTX, ctypes.POINTER(ctypes.c_int64)],
     "mag_reunitarize": [_CTX, _DP],
     "mag_stout_level": [_CTX, ctypes.c_int, ctypes.c_int, _DP],
     "mag_integrate": [_CTX],

@@ -18,6 +18,10 @@ struct DevGeom {
     const uint16_t* c2c;       // device array [vpad / MAG_CHUNK]
     long vpad;                 // padded global sites (multiple of MAG_CHUNK)
     int nchain;
+    // device array [nchain]: the chain's Philox stream index, added to a seed to form its
+    // key (default: the chain's position in the context; a sharded ensemble sets the
+    // chain's position in the whole ensemble)
+    const unsigned long long* stream_index;
 };
 
 // Per-trajectory record kept on the device, one per chain per trajectory.

@@ -271,7 +271,7 @@ __global__ void k_accept(DevGeom g, AcceptArgs a, const dd2* sums, ChainState* c
     r.plaq_new = dd_val(S[SLOT_PLAQ_NEW]);
     r.rect_old = dd_val(S[SLOT_RECT_OLD]);
     r.rect_new = dd_val(S[SLOT_RECT_NEW]);
-    const double u = a.uniform_override ? a.uniform_override[c] : uniform53(a.seed + (unsigned long long)c, (uint32_t)traj);
+    const double u = a.uniform_override ? a.uniform_override[c] : uniform53(a.seed + g.stream_index[c], (uint32_t)traj);
     r.uniform = u;
     ChainState st = cs[c];
     bool acc;
@@ -323,8 +323,9 @@ __global__ void k_momenta(DevGeom g, AlgPlanes<double> P, unsigned long long see
     const uint32_t link = (uint32_t)(4 * st.s + mu);
     const uint32_t traj = (uint32_t)(*traj_counter);
     double xi[8];
-    gauss4(seed + (unsigned long long)chain, link, 0u, traj, RNG_MOMENTA, xi);
-    gauss4(seed + (unsigned long long)chain, link, 1u, traj, RNG_MOMENTA, xi + 4);
+    const unsigned long long key = seed + g.stream_index[chain];
+    gauss4(key, link, 0u, traj, RNG_MOMENTA, xi);
+    gauss4(key, link, 1u, traj, RNG_MOMENTA, xi + 4);
     const double s2 = 1.0 / sqrt(2.0), s6 = 1.0 / sqrt(6.0);
     herm8<double> p;
     p.h[0] = xi[2] * s2 + xi[7] * s6;
@@ -347,7 +348,8 @@ __global__ void k_hot_start(DevGeom g, LinkPlanes<double> U, unsigned long long 
     const int chain = g.c2c[gs / MAG_CHUNK];
     const uint32_t link = (uint32_t)(4 * st.s + mu);
     double x[12];
-    for (int j = 0; j < 3; j++) gauss4(seed + (unsigned long long)chain, link, (uint32_t)j, 0u, RNG_HOT, x + 4 * j);
+    const unsigned long long key = seed + g.stream_index[chain];
+    for (int j = 0; j < 3; j++) gauss4(key, link, (uint32_t)j, 0u, RNG_HOT, x + 4 * j);
     mat3<double> m;
     for (int k = 0; k < 3; k++) {
         m.e[0][k] = mk(x[2 * k], x[2 * k + 1]);
@@ -474,6 +476,8 @@ template void launch_evolve<double, double>(const DevGeom&, LinkPlanes<double>, 
                                             AlgPlanes<double>, double, LinkPlanes<float>, cudaStream_t);
 template void launch_evolve<float, float>(const DevGeom&, LinkPlanes<float>, LinkPlanes<float>, AlgPlanes<float>,
                                           double, LinkPlanes<float>, cudaStream_t);
+template void launch_evolve<double, float>(const DevGeom&, LinkPlanes<double>, LinkPlanes<double>, AlgPlanes<float>,
+                                           double, LinkPlanes<float>, cudaStream_t);
 
 template <typename TF>
 void launch_kick(const DevGeom& g, AlgPlanes<double> P, AlgPlanes<TF> F, double eps, cudaStream_t s) {

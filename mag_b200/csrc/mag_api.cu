@@ -98,6 +98,7 @@ struct mag_ctx {
 
     ChainInfo* d_chains = nullptr;
     uint16_t* d_c2c = nullptr;
+    unsigned long long* d_stream_index = nullptr;
     LinkPlanes<double> U{nullptr, 0}, Ubak{nullptr, 0}, Uaux{nullptr, 0};
     AlgPlanes<double> P{nullptr, 0}, F{nullptr, 0};
     LinkPlanes<float> U32{nullptr, 0}, Uaux32{nullptr, 0};
@@ -241,7 +242,11 @@ struct mag_ctx {
                 c2c[k] = (uint16_t)c;
         MAG_CUDA(cudaMemcpy(d_chains, hc.data(), sizeof(ChainInfo) * n, cudaMemcpyHostToDevice));
         MAG_CUDA(cudaMemcpy(d_c2c, c2c.data(), sizeof(uint16_t) * nchunk, cudaMemcpyHostToDevice));
-        geom = DevGeom{d_chains, d_c2c, vpad, n};
+        MAG_TRY(alloc((void**)&d_stream_index, sizeof(unsigned long long) * n));
+        std::vector<unsigned long long> sidx(n);
+        for (int c = 0; c < n; c++) sidx[c] = (unsigned long long)c;
+        MAG_CUDA(cudaMemcpy(d_stream_index, sidx.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice));
+        geom = DevGeom{d_chains, d_c2c, vpad, n, d_stream_index};
 
         MAG_TRY(alloc_links(U));
         MAG_TRY(alloc_links(Ubak));
@@ -815,6 +820,31 @@ int mag_evolve_gauge(mag_ctx* ctx, double eps) {
     return ctx->sync("mag_evolve_gauge");
 }
 
+int mag_evolve_gauge_src(mag_ctx* ctx, double eps, int src) {
+    if (!ctx) return MAG_ERR_ARG;
+    if (src == MAG_SRC_MOMENTA) return mag_evolve_gauge(ctx, eps);
+    if (src != MAG_SRC_FORCE) return fail(MAG_ERR_ARG, "mag_evolve_gauge_src: src must be MAG_SRC_MOMENTA or MAG_SRC_FORCE");
+    // the force-gradient step's link update U <- exp(i eps F(U)) U (field-hmc.h:497-503)
+    if (ctx->mixed) {
+        ctx->force_eval<float>(ctx->U32, ctx->F32, ctx->st32);
+        launch_evolve<double, float>(ctx->geom, ctx->U, ctx->U, ctx->F32, eps, ctx->U32, ctx->stream);
+    } else {
+        ctx->force_eval<double>(ctx->U, ctx->F, ctx->st64);
+        launch_evolve<double, double>(ctx->geom, ctx->U, ctx->U, ctx->F, eps, LinkPlanes<float>{nullptr, 0},
+                                      ctx->stream);
+    }
+    return ctx->sync("mag_evolve_gauge_src");
+}
+
+int mag_stout_forward(mag_ctx* ctx, int chain, int level, double* host_aos) {
+    return mag_stout_level(ctx, chain, level, host_aos);
+}
+
+int mag_stout_force(mag_ctx* ctx, int chain, double* host_force_aos) {
+    if (ctx && ctx->p.n_stout < 1) return fail(MAG_ERR_STATE, "mag_stout_force: context has no stout levels");
+    return mag_gauge_force(ctx, chain, host_force_aos);
+}
+
 int mag_evolve_momentum(mag_ctx* ctx, double eps) {
     if (!ctx) return MAG_ERR_ARG;
     if (ctx->mixed) {
@@ -881,6 +911,16 @@ int mag_trajectory(mag_ctx* ctx, int refresh, mag_traj_result* results) {
     return MAG_OK;
 }
 
+int mag_fg_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results) {
+    return mag_trajectory(ctx, refresh_momenta, results);
+}
+
+int mag_batch_create(const mag_params* p, int n_chains, mag_ctx** out) {
+    return mag_ensemble_create(p, n_chains, out);
+}
+
+int mag_batch_run(mag_ctx* ctx, int n_traj, mag_traj_result* results) { return mag_run(ctx, n_traj, results); }
+
 int mag_run(mag_ctx* ctx, int n_traj, mag_traj_result* results) {
     if (!ctx || n_traj < 0) return MAG_ERR_ARG;
     MAG_TRY(ctx->build_graph());
@@ -911,6 +951,18 @@ int mag_run(mag_ctx* ctx, int n_traj, mag_traj_result* results) {
     ctx->last_run_ms = total;
     if (!finite) return fail(MAG_ERR_NAN, "non-finite Delta H");
     return MAG_OK;
+}
+
+int mag_set_stream_index(mag_ctx* ctx, const int64_t* index) {
+    if (!ctx || !index) return fail(MAG_ERR_ARG, "mag_set_stream_index: null argument");
+    std::vector<unsigned long long> v(ctx->nchain);
+    for (int c = 0; c < ctx->nchain; c++) {
+        if (index[c] < 0) return fail(MAG_ERR_ARG, "mag_set_stream_index: negative index");
+        v[c] = (unsigned long long)index[c];
+    }
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_stream_index, v.data(), sizeof(unsigned long long) * v.size(),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    return ctx->sync("mag_set_stream_index");
 }
 
 int mag_traj_counter(mag_ctx* ctx, int64_t* traj) {

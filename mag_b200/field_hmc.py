@@ -126,6 +126,11 @@ class Chmc:
         check(self._lib.mag_gauge_get(self._h, chain, _dp(U)), "mag_gauge_get")
         return U
 
+    def set_stream_index(self, index: Sequence[int]) -> None:
+        """Philox stream of each chain (key = seed + index[c]); see mag_set_stream_index."""
+        a = (ctypes.c_int64 * self.n_chains)(*[int(i) for i in index])
+        check(self._lib.mag_set_stream_index(self._h, a), "mag_set_stream_index")
+
     def hot_start(self, seed: int) -> None:
         check(self._lib.mag_gauge_hot_start(self._h, int(seed)), "mag_gauge_hot_start")
 
@@ -193,8 +198,14 @@ class Chmc:
         check(self._lib.mag_hamiltonian(self._h, chain, _dp(out)), "mag_hamiltonian")
         return float(out[0]), [float(out[1]), float(out[2])]
 
-    def evolve_gauge_field(self, dt: float) -> None:
-        check(self._lib.mag_evolve_gauge(self._h, float(dt)), "mag_evolve_gauge")
+    def evolve_gauge_field(self, dt: float, src: str = "momenta") -> None:
+        """evolve_gauge_field (field-hmc.h:442-482) with the momenta, or with the force of the
+        current links (src="force": the force-gradient step's U <- exp(i dt F(U)) U)."""
+        if src == "momenta":
+            check(self._lib.mag_evolve_gauge(self._h, float(dt)), "mag_evolve_gauge")
+        else:
+            code = {"force": 1}[src]
+            check(self._lib.mag_evolve_gauge_src(self._h, float(dt), code), "mag_evolve_gauge_src")
 
     def evolve_momentum(self, dt: float) -> None:
         check(self._lib.mag_evolve_momentum(self._h, float(dt)), "mag_evolve_momentum")

@@ -267,3 +267,66 @@ def test_nan_is_reported_as_error_status():
         with pytest.raises(M.MagError) as e:
             c.trajectory(True)
         assert e.value.code == -3
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_evolve_by_force_matches_oracle(precision):
+    """U <- exp(i dt F(U)) U (the force-gradient link update) against the oracle's
+    evolve_gauge driven by its own force; constrained Iwasaki with one stout level."""
+    U = O.gen_hot(DIMS, 31)
+    po = O.make_params(DIMS, mag=2, action=1, n_stout=1, rho=0.1)
+    with M.Chmc(DIMS, mag=2, action="iwasaki", n_stout=1, rho=0.1, precision=precision) as c:
+        c.set_gauge(U)
+        c.evolve_gauge_field(0.05, src="force")
+        Ug = c.get_gauge()
+    Uo = O.evolve_gauge(po, U, O.force(po, U), 0.05)
+    tol = 1e-12 if precision == "fp64" else 1e-6
+    assert np.abs(Ug - Uo).max() < tol
+
+
+def test_alias_entry_points():
+    """mag_stout_forward / mag_stout_force / mag_fg_trajectory / mag_batch_* are the same calls."""
+    import ctypes
+
+    from mag_b200 import _lib
+
+    L = _lib.load()
+    U = O.gen_hot(DIMS, 32)
+    with M.Chmc(DIMS, n_stout=2, rho=0.1, seed=4) as c:
+        c.set_gauge(U)
+        a = np.zeros_like(U)
+        _lib.check(L.mag_stout_forward(c._h, 0, 2, a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "sf")
+        assert np.array_equal(a, c.stout_level(2))
+        f = np.zeros_like(U)
+        _lib.check(L.mag_stout_force(c._h, 0, f.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "sF")
+        assert np.array_equal(f, c.get_force())
+        r = _lib.TrajResult()
+        _lib.check(L.mag_fg_trajectory(c._h, 1, ctypes.byref(r)), "fg")
+        assert np.isfinite(r.delta_h)
+    with M.Chmc(DIMS, n_stout=0) as c:
+        code = L.mag_stout_force(c._h, 0, np.zeros((O.volume(DIMS), 4, 3, 3), np.complex128).ctypes.data_as(
+            ctypes.POINTER(ctypes.c_double)))
+        assert code == _lib.MAG_ERR_STATE
+
+
+def test_split_ensemble_reproduces_the_single_context():
+    """Chains 0-3 in one context, or chains {0, 3} and {1, 2} in two contexts with their
+    ensemble stream indices: identical per-chain trajectories (bit for bit)."""
+    chains = [dict(dims=(4, 4, 4, 4), beta=2.1), dict(dims=(4, 4, 4, 6), beta=2.3),
+              dict(dims=(4, 4, 4, 4), beta=2.4), dict(dims=(4, 4, 6, 6), beta=2.2)]
+    kw = dict(n_stout=1, rho=0.1, n_steps=4, seed=17)
+    with M.Chmc(chains=chains, **kw) as c:
+        c.hot_start(17)
+        whole = c.run_chmc(3)
+        U_whole = [c.get_gauge(k) for k in range(4)]
+    for part in ([0, 3], [1, 2]):
+        with M.Chmc(chains=[chains[i] for i in part], **kw) as c:
+            c.set_stream_index(part)
+            c.hot_start(17)
+            rec = c.run_chmc(3)
+            for j, i in enumerate(part):
+                for t in range(3):
+                    assert rec[t][j]["delta_h"] == whole[t][i]["delta_h"]
+                    assert rec[t][j]["accept"] == whole[t][i]["accept"]
+                assert np.array_equal(c.get_gauge(j), U_whole[i])
+

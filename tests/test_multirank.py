@@ -62,3 +62,60 @@ def test_single_process_needs_no_group():
     import bench
 
     assert bench.max_over_ranks(3.0, None, "cpu") == 3.0
+
+
+def test_partition_balances_the_ensemble():
+    import bench
+    from mag_b200.ensemble import chain_cost, imbalance, partition
+
+    chains = bench.workload_params("ensemble_96chains")["chains"]
+    costs = [chain_cost(c["dims"], 8) for c in chains]
+    for world in (1, 2, 3, 4, 8):
+        parts = partition(costs, world)
+        flat = sorted(i for p in parts for i in p)
+        assert flat == list(range(len(chains)))                     # every chain exactly once
+        assert parts == partition(costs, world)                     # the same split on every rank
+        assert imbalance(costs, parts) < 1.0 + max(costs) / (sum(costs) / world)  # LPT bound
+    assert imbalance(costs, partition(costs, 2)) < 1.01
+    assert imbalance(costs, partition(costs, 8)) < 1.1
+
+
+def _gather_worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        from mag_b200.ensemble import gather_records, partition
+
+        costs = [5, 1, 4, 2, 3, 3, 1]
+        parts = partition(costs, world)
+        # trajectory t of global chain c: delta_h = 100 t + c, accept = c % 2
+        recs = [[{"delta_h": 100.0 * t + c, "accept": c % 2, "avg_plaquette": 0.5 + c, "h_old": 1.0, "h_new": 2.0,
+                  "uniform": 0.25, "reunit_maxdev": 0.0} for c in parts[rank]] for t in range(3)]
+        out = gather_records(recs, parts, rank, dist, "cpu")
+        q.put((rank, [[(r["delta_h"], r["accept"]) for r in row] for row in out], parts))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_records_over_two_gloo_ranks():
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_gather_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    res = sorted(q.get(timeout=10) for _ in range(world))
+    expect = [[(100.0 * t + c, c % 2) for c in range(7)] for t in range(3)]
+    assert res[0][1] == expect and res[1][1] == expect
+    assert res[0][2][0] and res[0][2][1]   # both ranks hold chains
+
