@@ -620,17 +620,17 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
     if (q2 > 9.f) return false;
     float a = 1.f, b = 0.f, d = 0.f;                       // Q^n coefficients
     float a0 = 0.f, b0 = 0.f, d0 = 0.f, a1 = 0.f, b1 = 0.f, d1 = 0.f;  // d/dc0, d/dc1
-    float F[3][2] = {{1.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};  // f_j (re, im); n = 0 term
-    float B1[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
-    float B2[3][2] = {{0.f, 0.f}, {0.f, 0.f}, {0.f, 0.f}};
+    // f_j and the b coefficients, real and imaginary parts apart (n = 0 term: f_0 = 1)
+    float Fr[3] = {1.f, 0.f, 0.f}, Fi[3] = {0.f, 0.f, 0.f};
+    float B1r[3] = {0.f, 0.f, 0.f}, B1i[3] = {0.f, 0.f, 0.f};
+    float B2r[3] = {0.f, 0.f, 0.f}, B2i[3] = {0.f, 0.f, 0.f};
     float coef = 1.f;    // 1/n!
     float bound = 1.f;   // q^n / n! for q >= 1, q^(n-5) / n! for q < 1: the a_n, b_n, d_n
                          // and their derivatives carry powers of q down to q^(n-5)
     const float q = sqrtf(q2);
     const bool qbig = q >= 1.f;
-#pragma unroll 1
-    for (int n = 1; n < 40; n++) {
-        // advance Q^{n-1} -> Q^n (and the derivatives)
+    // one term: advance Q^{n-1} -> Q^n (and the derivatives), add i^n/n! times it
+    auto term = [&](int n, bool odd) {
         const float na = c0 * d, nb = a + c1 * d, nd = b;
         if (WITH_B) {
             const float na0 = d + c0 * d0, nb0 = a0 + c1 * d0, nd0 = b0;
@@ -641,21 +641,29 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
         a = na; b = nb; d = nd;
         coef /= (float)n;
         bound *= (qbig || n > 5 ? q : 1.f) / (float)n;
-        // i^n/n!: real for even n (sign (-1)^{n/2}), imaginary for odd n
-        const int part = n & 1;
-        const float s = ((n >> 1) & 1) ? -coef : coef;
-        F[0][part] += s * a;
-        F[1][part] += s * b;
-        F[2][part] += s * d;
+        // i^n/n!: real for even n (sign (-1)^{n/2}), imaginary for odd n (sign (-1)^{(n-1)/2})
+        const float sgn = ((n >> 1) & 1) ? -coef : coef;
+        float* F = odd ? Fi : Fr;
+        F[0] = fmaf(sgn, a, F[0]);
+        F[1] = fmaf(sgn, b, F[1]);
+        F[2] = fmaf(sgn, d, F[2]);
         if (WITH_B) {
-            B1[0][part] += s * a1; B1[1][part] += s * b1; B1[2][part] += s * d1;
-            B2[0][part] += s * a0; B2[1][part] += s * b0; B2[2][part] += s * d0;
+            float* P = odd ? B1i : B1r;
+            float* R = odd ? B2i : B2r;
+            P[0] = fmaf(sgn, a1, P[0]); P[1] = fmaf(sgn, b1, P[1]); P[2] = fmaf(sgn, d1, P[2]);
+            R[0] = fmaf(sgn, a0, R[0]); R[1] = fmaf(sgn, b0, R[1]); R[2] = fmaf(sgn, d0, R[2]);
         }
-        if (n > 5 && bound < 1e-9f) break;
+    };
+    // terms in pairs (odd, even) so that the real / imaginary choice is known at compile time
+#pragma unroll 1
+    for (int n = 1; n < 40; n += 2) {
+        term(n, true);
+        term(n + 1, false);
+        if (n + 1 > 5 && bound < 1e-9f) break;
     }
-    r.f0r = F[0][0]; r.f0i = F[0][1]; r.f1r = F[1][0]; r.f1i = F[1][1]; r.f2r = F[2][0]; r.f2i = F[2][1];
-    r.b10r = B1[0][0]; r.b10i = B1[0][1]; r.b11r = B1[1][0]; r.b11i = B1[1][1]; r.b12r = B1[2][0]; r.b12i = B1[2][1];
-    r.b20r = B2[0][0]; r.b20i = B2[0][1]; r.b21r = B2[1][0]; r.b21i = B2[1][1]; r.b22r = B2[2][0]; r.b22i = B2[2][1];
+    r.f0r = Fr[0]; r.f0i = Fi[0]; r.f1r = Fr[1]; r.f1i = Fi[1]; r.f2r = Fr[2]; r.f2i = Fi[2];
+    r.b10r = B1r[0]; r.b10i = B1i[0]; r.b11r = B1r[1]; r.b11i = B1i[1]; r.b12r = B1r[2]; r.b12i = B1i[2];
+    r.b20r = B2r[0]; r.b20i = B2i[0]; r.b21r = B2r[1]; r.b21i = B2i[1]; r.b22r = B2r[2]; r.b22i = B2i[2];
     return true;
 }
 
