@@ -74,7 +74,9 @@ __device__ dd2 block_reduce(dd2 v) {
 
 // ------------------------------------------------------------------- updates
 template <typename TU, typename TX>
-__global__ void k_evolve(DevGeom g, LinkPlanes<TU> Uin, LinkPlanes<TU> Uout, AlgPlanes<TX> X, double eps,
+// two resident blocks per SM (at most 128 registers): a streaming kernel needs the warps
+__global__ void __launch_bounds__(kBlock, 2) k_evolve(DevGeom g, LinkPlanes<TU> Uin, LinkPlanes<TU> Uout,
+                                                      AlgPlanes<TX> X, double eps,
                          LinkPlanes<float> Ucopy) {
     ChainInfo ci;
     Site st;
