@@ -51,8 +51,11 @@ WORKLOADS = {
     "16x16x16x32_iwasaki_3stout": dict(dims=(16, 16, 16, 32), beta=2.25, n_stout=3, n_steps=12, precision="fp64"),
     # 32^4, 3 stout levels, 16 FG steps: FP64 with the mixed-precision leg beside it
     "32x32x32x32_iwasaki_3stout": dict(dims=(32, 32, 32, 32), beta=2.25, n_stout=3, n_steps=16, precision="fp64"),
-    # 8^4 thin-link Iwasaki, 8 FG steps (the CPU-runnable configuration)
-    "8x8x8x8_iwasaki_thin": dict(dims=(8, 8, 8, 8), beta=2.25, n_stout=0, n_steps=8, precision="fp64"),
+    # 8^4 thin-link Iwasaki, 8 FG steps, demon accept with the demons started at 0 (the CPU-runnable
+    # configuration); E_max = 1e5 in units of sum ReTr lets the demons absorb the action change of a hot
+    # start (about 7e3 on the first trajectories; with the default 100 every trajectory is rejected)
+    "8x8x8x8_iwasaki_thin": dict(dims=(8, 8, 8, 8), beta=2.25, n_stout=0, n_steps=8, precision="fp64",
+                                 accept="demon", e_max=1e5),
     # 96 chains in one context, 1 stout level, 8 FG steps, mixed precision
     "ensemble_96chains": dict(chains="ensemble", n_stout=1, n_steps=8, precision="mixed"),
     # 48^3 x 96, beta 2.37, 3 stout levels, 16 FG steps, mixed, Wilson loops R, T <= 8 after each trajectory
@@ -290,7 +293,7 @@ def reference_arm(args, params, rank: int, world: int):
 def config_of(name, params, world, shard=False):
     c = {"workload": name, "action": "iwasaki", "c1": params["c1"], "stout_levels": params["n_stout"],
          "rho": params["rho"], "fg_steps": params["n_steps"], "tau": params["tau"], "mag": params["mag"],
-         "precision": params["precision"], "accept": "metropolis",
+         "precision": params["precision"], "accept": params.get("accept", "metropolis"),
          "parallelism": f"chains split over {world} GPUs" if shard else f"replicas{world}",
          "l2": "working set > 126 MB L2 (links, momenta, stout levels)"}
     if "chains" in params:

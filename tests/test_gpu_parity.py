@@ -166,6 +166,20 @@ def test_trajectory_parity_three_stout_levels():
         assert du < 1e-10
 
 
+@pytest.mark.slow
+def test_trajectory_parity_16x16x16x32_three_stout_full_size():
+    """The FP64 GPU configuration at its full size: 16^3 x 32, Iwasaki beta = 2.25, three
+    stout levels rho = 0.1, twelve force-gradient steps, one trajectory against the oracle
+    (about 100 s of oracle time on 16 host threads)."""
+    res = _run_pair((16, 16, 16, 32), dict(mag=2, n_stout=3, rho=0.1, n_steps=12), 1)
+    g, o, du = res[0]
+    assert abs(g["h_old"] - o["h_old"]) <= 1e-12 * abs(o["h_old"])
+    assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
+    assert g["accept"] == o["accept"]
+    assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-12
+    assert du < 1e-10
+
+
 def test_leapfrog_parity():
     res = _run_pair((4, 4, 4, 4), dict(mag=0, n_steps=6, integrator="leapfrog"), 1)
     g, o, du = res[0]
