@@ -168,6 +168,22 @@ int mag_set_stream_index(mag_ctx* ctx, const int64_t* index);
 int mag_traj_counter(mag_ctx* ctx, int64_t* traj);
 int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);
 
+/* --------------------------------------------------- per-link demon sweep */
+/* demon_microcanonical (field-demon.h:25-126) on one chain: n_sweeps sweeps over
+   the links in site order (x0 fastest, mu inner) of a copy of the links, each link
+   with its plaquette, rectangle, chair and twist staples (field-hmc.h:137-242,
+   field-staple.h:27-149) and two hits of random_su3_from_su2(0.9) (field-matrix.h:36-65,
+   drawn from Philox with this seed); a hit is accepted iff all four demons stay
+   inside (-e_max, e_max).  The demons start at 0; after every sweep the field is
+   reunitarized.  demon_energy[4 * i + k] = demon k after sweep i, reunit[i] = the
+   reunitarisation's maximum deviation (either may be NULL); accepted / rejected count
+   the hits.  update_links = 0 leaves the context's links as they were (the reference
+   sweeps a copy); 1 keeps the swept field.  The sweep is sequential: one CTA walks
+   the links, each link's 168 staple paths computed in parallel. */
+int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max, uint64_t seed,
+                             int update_links, double* demon_energy, int64_t* accepted, int64_t* rejected,
+                             double* reunit);
+
 /* ------------------------------------------------------------ measurement */
 /* avg_wilson_loop (field-wloop.h:58-99) for a general spatial vector r and extent T */
 int mag_wilson_loop(mag_ctx* ctx, int chain, const int r[3], int T, double* out);

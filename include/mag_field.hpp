@@ -171,6 +171,31 @@ inline double avg_wilson_loop(Lattice& L, const std::array<int, 3>& r, int T) {
     return v;
 }
 
+// ------------------------------------------------------------ field-demon.h
+// demon_microcanonical (field-demon.h:25-126): arg.num_trajectory sweeps of the
+// per-link demons over a copy of the links (the lattice keeps its links).  When
+// `summary` is given, the four demon energies of sweep i are appended to it as
+// doubles for i >= num_step_before_output and i % num_step_between_output == 0, the
+// record the reference writes to demon_equil<info>.dat.  Returns the energies of
+// every sweep (4 per sweep).
+inline std::vector<double> demon_microcanonical(Lattice& L, double E_max, uint64_t seed = 1,
+                                                FILE* summary = nullptr, int64_t* accepted = nullptr,
+                                                int64_t* rejected = nullptr) {
+    const int n = L.arg().num_trajectory;
+    std::vector<double> E((size_t)4 * n);
+    std::vector<double> dev((size_t)n);
+    check(mag_demon_microcanonical(L.ctx(), 0, n, E_max, seed, 0, E.data(), accepted, rejected, dev.data()),
+          "demon_microcanonical");
+    if (summary) {
+        const int every = L.arg().num_step_between_output > 0 ? L.arg().num_step_between_output : 1;
+        for (int i = 0; i < n; i++)
+            if (i >= L.arg().num_step_before_output && i % every == 0)
+                std::fwrite(E.data() + 4 * i, sizeof(double), 4, summary);
+        std::fflush(summary);
+    }
+    return E;
+}
+
 // ---------------------------------------------------- field-matrix.h NERSC I/O
 // Arg_export (field-matrix.h:445-450)
 struct Arg_export {

@@ -158,6 +158,18 @@ void launch_payload_to_links(const double* payload, int two_row, int off, int V,
                              cudaStream_t s);
 void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s);
 
+// ---- per-link demon sweep (kernels_demon.cu)
+constexpr int kDemonPaths = 168;  // staple paths per link: 6 plaquette, 18 rectangle, 72 chair, 72 twist
+struct DemonState {
+    double E[4];  // plaquette, rectangle, chair, twist demons
+    long long accept, reject;
+};
+// path table [4 mu][kDemonPaths][5] (0-3 forward, 4-7 backward, -1 padding)
+void build_demon_paths(int8_t* out);
+// one sweep over the links of one chain (a single CTA, links in site order)
+void launch_demon_sweep(const ChainInfo& ci, LinkPlanes<double> U, const int8_t* paths, unsigned long long seed,
+                        int sweep, double e_max, DemonState* st, cudaStream_t s);
+
 // ---- measurements (kernels_wloop.cu)
 // planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;
 // out[((i * Tmax + T-1) * nchain + c) * Rmax + R-1] (i = spatial direction)

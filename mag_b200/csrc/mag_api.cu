@@ -120,6 +120,8 @@ struct mag_ctx {
     long max_v = 0;
     // NERSC I/O: pinned double buffer, CRC segment registers, word checksum
     nersc::Pinned pin;
+    int8_t* d_demon_paths = nullptr;  // per-link demon sweep: staple path table
+    DemonState* d_demon = nullptr;
     uint32_t* d_crc = nullptr;      // segment registers (kCrcThreads + 1)
     uint32_t* d_crc2 = nullptr;     // folded groups
     uint32_t* d_crc_tab = nullptr;  // 4 x 256 shift tables of one segment
@@ -909,6 +911,57 @@ int mag_trajectory(mag_ctx* ctx, int refresh, mag_traj_result* results) {
     }
     if (!finite) return fail(MAG_ERR_NAN, "non-finite Delta H");
     return MAG_OK;
+}
+
+int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max, uint64_t seed,
+                             int update_links, double* demon_energy, int64_t* accepted, int64_t* rejected,
+                             double* reunit) {
+    if (!ctx || n_sweeps < 0 || !(e_max >= 0.0)) return fail(MAG_ERR_ARG, "mag_demon_microcanonical: bad argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    if (!ctx->d_demon_paths) {
+        std::vector<int8_t> table((size_t)4 * kDemonPaths * 5);
+        build_demon_paths(table.data());
+        MAG_TRY(ctx->alloc((void**)&ctx->d_demon_paths, table.size()));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_demon, sizeof(DemonState)));
+        MAG_CUDA(cudaMemcpy(ctx->d_demon_paths, table.data(), table.size(), cudaMemcpyHostToDevice));
+    }
+    // the reference sweeps a copy of the field (field-demon.h:47-49) and starts the demons at 0 (:44);
+    // the copy lives in the reject backup, which only a trajectory in progress uses
+    const DemonState zero{{0.0, 0.0, 0.0, 0.0}, 0, 0};
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_demon, &zero, sizeof(zero), cudaMemcpyHostToDevice, ctx->stream));
+    LinkPlanes<double> work = ctx->Ubak;
+    launch_link_copy(ctx->geom, ctx->U, work, ctx->stream);
+    for (int i = 0; i < n_sweeps; i++) {
+        launch_demon_sweep(ctx->hc[chain], work, ctx->d_demon_paths, seed, i, e_max, ctx->d_demon, ctx->stream);
+        // field-demon.h:111 reunitarizes the swept field after every sweep
+        MAG_CUDA(cudaMemsetAsync(ctx->reunit, 0, sizeof(unsigned long long) * ctx->nchain, ctx->stream));
+        launch_reunitarize(ctx->geom, work, LinkPlanes<float>{nullptr, 0}, ctx->reunit, ctx->stream);
+        DemonState st;
+        unsigned long long bits = 0;
+        MAG_CUDA(cudaMemcpyAsync(&st, ctx->d_demon, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
+        MAG_CUDA(cudaMemcpyAsync(&bits, ctx->reunit + chain, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+        MAG_TRY(ctx->sync("mag_demon_microcanonical"));
+        if (demon_energy)
+            for (int k = 0; k < 4; k++) demon_energy[4 * i + k] = st.E[k];
+        if (reunit) {
+            double d;
+            memcpy(&d, &bits, sizeof(d));
+            reunit[i] = d;
+        }
+        if (i == n_sweeps - 1) {
+            if (accepted) *accepted = st.accept;
+            if (rejected) *rejected = st.reject;
+        }
+    }
+    if (n_sweeps == 0) {
+        if (accepted) *accepted = 0;
+        if (rejected) *rejected = 0;
+    }
+    if (update_links) {
+        launch_link_copy(ctx->geom, work, ctx->U, ctx->stream);
+        MAG_TRY(ctx->refresh_copy());
+    }
+    return ctx->sync("mag_demon_microcanonical");
 }
 
 int mag_fg_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results) {

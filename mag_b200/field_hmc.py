@@ -264,6 +264,21 @@ class Chmc:
         check(self._lib.mag_constrained_plaquette(self._h, chain, ctypes.byref(v)), "mag_constrained_plaquette")
         return v.value
 
+    # ------------------------------------------------------------ demon sweep
+    def demon_microcanonical(self, n_sweeps: int, e_max: float, seed: int = 1, update_links: bool = False,
+                             chain: int = 0) -> dict:
+        """demon_microcanonical (field-demon.h:25-126): per-link demon sweeps with plaquette,
+        rectangle, chair and twist demons.  Returns the demon energies after each sweep
+        ([n_sweeps, 4]), the accepted / rejected hit counts and the reunitarisation deviation
+        of each sweep."""
+        E = np.zeros((int(n_sweeps), 4))
+        dev = np.zeros(int(n_sweeps))
+        a, r = ctypes.c_int64(), ctypes.c_int64()
+        check(self._lib.mag_demon_microcanonical(self._h, chain, int(n_sweeps), float(e_max), int(seed),
+                                                 1 if update_links else 0, _dp(E), ctypes.byref(a),
+                                                 ctypes.byref(r), _dp(dev)), "mag_demon_microcanonical")
+        return {"demon_energy": E, "accepted": a.value, "rejected": r.value, "reunit_maxdev": dev}
+
     # ------------------------------------------------------------ NERSC I/O
     def export_config_nersc(self, path: str, beta: float | None = None, sequence_num: int = 0,
                             ensemble_label: str = "", skip_third: bool = True, chain: int = 0) -> dict:

@@ -102,6 +102,8 @@ def lib():
             "mo_wilson_loop": (ctypes.c_double, [ip, dp, ip, ctypes.c_int]),
             "mo_constrained_plaquette": (ctypes.c_double, [ip, dp, ctypes.c_int]),
             "mo_gauge_transform": (None, [ip, dp, dp]),
+            "mo_demon_sweeps": (None, [ip, dp, ctypes.c_uint64, ctypes.c_int, ctypes.c_double, dp,
+                                       ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), dp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -307,3 +309,16 @@ def gauge_transform(dims, U, G):
     U = U.copy()
     lib().mo_gauge_transform(_dims(dims), _dp(U), _dp(_m(G)))
     return U
+
+
+def demon_sweeps(dims, U, seed: int, n_sweeps: int, e_max: float):
+    """field-demon.h:25-126 demon_microcanonical: returns (U after the sweeps, demon
+    energies [n_sweeps, 4], accepted hits, rejected hits, reunitarize deviation per sweep)."""
+    U = np.ascontiguousarray(U, np.complex128).copy()
+    E = np.zeros((n_sweeps, 4))
+    dev = np.zeros(n_sweeps)
+    a, r = ctypes.c_int64(), ctypes.c_int64()
+    lib().mo_demon_sweeps(_dims(dims), _dp(U), int(seed), int(n_sweeps), float(e_max), _dp(E), ctypes.byref(a),
+                          ctypes.byref(r), _dp(dev))
+    return U, E, a.value, r.value, dev
+

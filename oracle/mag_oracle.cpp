@@ -1075,3 +1075,132 @@ void mo_gauge_transform(const int dims[4], double* U, const double* G) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------- per-link demon sweep
+namespace {
+
+enum { PURPOSE_DEMON_SU2 = 4, PURPOSE_DEMON_SUBGROUP = 5 };
+
+// field-staple.h:27-72 (init_chair_index) and :74-120 (init_twist_index): for every
+// nu != mu and lambda not in {mu, nu}, four four-step base paths, each with mu
+// inserted before step 1, 2 or 3 (72 five-step paths per mu); 0-3 forward,
+// 4-7 backward.  The lists are rebuilt here step by step as the reference builds them.
+std::vector<std::vector<int>> demon_paths(int mu, bool twist) {
+    std::vector<std::vector<int>> out;
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        for (int la = 0; la < 4; la++) {
+            if (la == nu || la == mu) continue;
+            int base[4][4];
+            if (!twist) {
+                const int b[4][4] = {{nu, la, la + 4, nu + 4}, {nu, la + 4, la + 4, nu},
+                                     {nu + 4, la, la, nu + 4}, {nu + 4, la + 4, la, nu}};
+                std::memcpy(base, b, sizeof(b));
+            } else {
+                const int b[4][4] = {{nu, la, nu + 4, la + 4}, {nu, la + 4, nu + 4, la},
+                                     {nu + 4, la, nu, la + 4}, {nu + 4, la + 4, nu, la}};
+                std::memcpy(base, b, sizeof(b));
+            }
+            for (int k = 0; k < 4; k++)
+                for (int i = 1; i < 4; i++) {
+                    std::vector<int> d(base[k], base[k] + 4);
+                    d.insert(d.begin() + i, mu);
+                    out.push_back(d);
+                }
+        }
+    }
+    return out;
+}
+
+// field-staple.h:125-134 chair_staple_dagger / :140-149 twist_staple_dagger: the
+// plain sum of the path products (no dagger, despite the name)
+M3 demon_staple(const Field& f, const int x[4], const std::vector<std::vector<int>>& paths) {
+    M3 acc = zero3();
+    for (const auto& d : paths) acc = acc + path_product(f, x, d.data(), (int)d.size());
+    return acc;
+}
+
+inline double u32(uint32_t v) { return ((double)v + 0.5) * 2.3283064365386963e-10; }
+
+// field-matrix.h:36-65 random_su3_from_su2(small, rng): a0 uniform in [small, 1),
+// a1..a3 uniform in [-1, 1) scaled to |a| = sqrt(1 - a0^2), embedded in the SU(2)
+// subgroup rand_gen % 3; the draws come from Philox counters (link, sweep, hit).
+M3 random_su3_from_su2(double small, uint64_t seed, uint32_t link, uint32_t sweep, uint32_t hit) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    const uint32_t c1[4] = {link, sweep, hit, PURPOSE_DEMON_SU2};
+    const uint32_t c2[4] = {link, sweep, hit, PURPOSE_DEMON_SUBGROUP};
+    uint32_t o[4], q[4];
+    philox(c1, key, o);
+    philox(c2, key, q);
+    const double a0 = small + (1.0 - small) * u32(o[0]);
+    double a1 = -1.0 + 2.0 * u32(o[1]), a2 = -1.0 + 2.0 * u32(o[2]), a3 = -1.0 + 2.0 * u32(o[3]);
+    const double norm = std::sqrt((1. - a0 * a0) / (a1 * a1 + a2 * a2 + a3 * a3));
+    a1 *= norm; a2 *= norm; a3 *= norm;
+    M3 m = unit3();
+    int i = 0, j = 0;
+    switch (q[0] % 3) {
+        case 0: i = 1; j = 2; break;
+        case 1: i = 0; j = 2; break;
+        default: i = 0; j = 1; break;
+    }
+    set(m, i, i, cplx(a0, a3));
+    set(m, i, j, cplx(a2, a1));
+    set(m, j, i, cplx(-a2, a1));
+    set(m, j, j, cplx(a0, -a3));
+    return m;
+}
+
+}  // namespace
+
+extern "C" {
+
+// field-demon.h:25-126 demon_microcanonical on a copy of the links: sites in index
+// order, mu = 0..3, plaquette / rectangle / chair / twist staples of the current
+// field, two hits of random_su3_from_su2(0.9), accept iff every demon stays in
+// (-E_max, E_max); after each sweep the demons are recorded and the field is
+// reunitarized (field-demon.h:111).  E starts at 0 (field-demon.h:44).
+void mo_demon_sweeps(const int dims[4], double* U, uint64_t seed, int n_sweeps, double e_max, double* E_trace,
+                     int64_t* accept, int64_t* reject, double* reunit) {
+    Lat lat(dims);
+    Field f{&lat, U};
+    std::vector<std::vector<int>> chairs[4], twists[4];
+    for (int mu = 0; mu < 4; mu++) {
+        chairs[mu] = demon_paths(mu, false);
+        twists[mu] = demon_paths(mu, true);
+    }
+    double E[4] = {0.0, 0.0, 0.0, 0.0};
+    int64_t acc = 0, rej = 0;
+    for (int i = 0; i < n_sweeps; i++) {
+        for (long s = 0; s < lat.V; s++) {
+            int x[4];
+            lat.coord(s, x);
+            for (int mu = 0; mu < 4; mu++) {
+                const M3 S[4] = {staple_dagger(f, x, mu), rect_dagger(f, x, mu), demon_staple(f, x, chairs[mu]),
+                                 demon_staple(f, x, twists[mu])};
+                for (int n = 0; n < 2; n++) {
+                    const M3 m = random_su3_from_su2(0.9, seed, (uint32_t)(4 * s + mu), (uint32_t)i, (uint32_t)n);
+                    M3& v = f.at(s, mu);
+                    double dS[4];
+                    bool ok = true;
+                    for (int k = 0; k < 4; k++) {
+                        dS[k] = -retr((m * v) * S[k]) + retr(v * S[k]);
+                        ok = ok && E[k] - dS[k] > -e_max && E[k] - dS[k] < e_max;
+                    }
+                    if (ok) {
+                        v = m * v;
+                        for (int k = 0; k < 4; k++) E[k] -= dS[k];
+                        acc++;
+                    } else {
+                        rej++;
+                    }
+                }
+            }
+        }
+        for (int k = 0; k < 4; k++) E_trace[4 * i + k] = E[k];
+        reunit[i] = reunitarize(lat, U);
+    }
+    *accept = acc;
+    *reject = rej;
+}
+
+}  // extern "C"

@@ -87,6 +87,10 @@ double mo_wilson_loop(const int dims[4], const double* U, const int r[3], int T)
 double mo_constrained_plaquette(const int dims[4], const double* U, int mag);
 void mo_gauge_transform(const int dims[4], double* U, const double* G);
 
+// field-demon.h:25-126 demon_microcanonical (per-link demons) on U in place
+void mo_demon_sweeps(const int dims[4], double* U, uint64_t seed, int n_sweeps, double e_max, double* E_trace,
+                     int64_t* accept, int64_t* reject, double* reunit);
+
 #ifdef __cplusplus
 }
 #endif

@@ -289,3 +289,20 @@ def test_trajectory_metropolis_and_demon_rules():
     pz = O.make_params(dims, mag=2, n_steps=4, accept=1, e_max=1e-6)
     Uz, rz = O.trajectory(pz, 0, U, P, 0.0, [0.0, 0.0])
     assert rz["accept"] == 0 and rz["demon"] == [0.0, 0.0] and np.array_equal(Uz, U)
+
+
+def test_demon_sweep_conserves_plaquette_and_rectangle_energy():
+    """field-demon.h:25-126: the plaquette and rectangle demons absorb exactly the change
+    of the total plaquette / rectangle sums (E_k = -sum dS_k, dS = the action change of
+    the loops through the updated link), up to the reunitarisation after each sweep."""
+    dims = (4, 4, 4, 4)
+    U = O.gen_hot(dims, 3)
+    p0, r0 = O.plaq_rect(dims, U)
+    U1, E, acc, rej, dev = O.demon_sweeps(dims, U, seed=7, n_sweeps=2, e_max=50.0)
+    p1, r1 = O.plaq_rect(dims, U1)
+    assert acc + rej == 2 * 2 * 4 * O.volume(dims) and acc > 0 and rej > 0
+    assert abs(E[-1, 0] - (p1 - p0)) < 1e-9 and abs(E[-1, 1] - (r1 - r0)) < 1e-9
+    assert np.all(np.abs(E) < 50.0) and np.all(dev < 1e-13)
+    # the demons never leave the window; with a zero window nothing is accepted
+    _, E0, acc0, rej0, _ = O.demon_sweeps(dims, U, seed=7, n_sweeps=1, e_max=0.0)
+    assert acc0 == 0 and np.all(E0 == 0.0)
