@@ -65,6 +65,10 @@ WORKLOADS = {
     # a step is one load from the page cache; the save (export_config_nersc) is timed beside it
     "nersc_io_32x32x32x32": dict(dims=(32, 32, 32, 32), beta=2.25, n_stout=0, n_steps=1, precision="fp64",
                                  kind="nersc"),
+    # per-link demon microcanonical sweeps (demon_microcanonical) of an 8^4 hot start, E_max = 50;
+    # a step is one sweep over the 16384 links (sequential by definition)
+    "demon_8x8x8x8": dict(dims=(8, 8, 8, 8), beta=2.25, n_stout=0, n_steps=1, precision="fp64", kind="demon",
+                          e_max=50.0),
 }
 DEFAULT = "16x16x16x32_iwasaki_3stout"
 COMMON = dict(mag=2, action="iwasaki", c1=-0.331, rho=0.1, tau=1.0, accept="metropolis", integrator="fg")
@@ -676,6 +680,110 @@ def run_nersc(args, params, rank, world, dist):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- demon sweep workload
+DEMON_METRIC = "per-link demon sweeps/s (demon_microcanonical, link updates/s = 4 V sweeps/s)"
+# flops of one link: 6 plaquette paths (2 products), 162 five-link paths (4 products), 198 per
+# product, and two hits of 3 products on each of 4 demons
+DEMON_FLOPS_PER_LINK = (6 * 2 + 162 * 4) * 198 + 2 * 4 * 3 * 198
+
+
+def demon_config(args, params, world):
+    return {"workload": args.workload, "lattice": "x".join(str(d) for d in params["dims"]),
+            "e_max": params["e_max"], "hits_per_link": 2, "demons": "plaquette, rectangle, chair, twist",
+            "parallelism": f"replicas{world}", "l2": "8^4 links (4.7 MB) stay in L2: one sweep is latency-bound"}
+
+
+def demon_reference_arm(args, params, rank: int, world: int):
+    """The oracle's sequential restatement (one host thread: the sweep is sequential)."""
+    if rank != 0:
+        return
+    import oracle as O
+
+    dims = params["dims"]
+    U = O.gen_hot(dims, 1)
+    for _ in range(args.warmup):
+        O.demon_sweeps(dims, U, 1, 1, params["e_max"])
+    ts = []
+    for i in range(args.steps):
+        t0 = time.perf_counter()
+        O.demon_sweeps(dims, U, 1 + i, 1, params["e_max"])
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    line = {"metric": DEMON_METRIC, "value": 1.0 / t, "unit": "sweeps/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
+            "config": demon_config(args, params, world),
+            "cpu_baseline": {"value": 1.0 / t, "unit": "sweeps/s", "cores": 1, "kind": "port",
+                             "sample": f"one sweep over the {4 * site_count(dims)} links per step"},
+            "e2e": {"value": 1.0 / t, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_demon(args, params, rank, world, dist):
+    import torch
+
+    import mag_b200 as M
+    from mag_b200.field_hmc import probe_fma_peak
+
+    dims = params["dims"]
+    V = site_count(dims)
+    seed = rank_seed(rank)
+    with M.Chmc(dims, mag=0, beta=params["beta"], n_stout=0, seed=seed) as c:
+        c.hot_start(seed)
+        c.demon_microcanonical(args.warmup, params["e_max"], seed=seed)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(gpu_index_for_smi()) if rank == 0 else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = c.demon_microcanonical(args.steps, params["e_max"], seed=seed + 1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        dev_s = c.last_measure_ms() / 1e3  # CUDA events on the library's stream around the sweeps
+        clocks = sampler.stop() if sampler else None
+    el = max_over_ranks(dev_s, dist, "cuda")
+    wall = max_over_ranks(wall, dist, "cuda")
+    if rank != 0:
+        return
+    sweep_s = el / args.steps
+    flops = DEMON_FLOPS_PER_LINK * 4 * V / sweep_s / 1e12
+    sm_peak = probe_fma_peak("fp64") / 148.0
+    cpu = None
+    if not args.no_cpu:
+        import oracle as O
+
+        U = O.gen_hot(dims, 1)
+        t0 = time.perf_counter()
+        O.demon_sweeps(dims, U, 1, 1, params["e_max"])
+        tc = time.perf_counter() - t0
+        cpu = {"value": 1.0 / tc, "unit": "sweeps/s", "cores": 1, "kind": "port",
+               "sample": f"one sweep of the oracle over the {4 * V} links (sequential, one host thread)"}
+    line = {
+        "metric": DEMON_METRIC, "value": world / sweep_s, "unit": "sweeps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sweep_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
+        "config": demon_config(args, params, world),
+        "link_updates_per_s": world * 4 * V / sweep_s,
+        "accepted": res["accepted"], "rejected": res["rejected"],
+        "roofline": {"bound": "fp64 (one SM: the sweep is one CTA)", "achieved": flops, "peak": sm_peak,
+                     "unit": "TFLOP/s", "frac": flops / sm_peak, "traffic": None,
+                     "flops_per_link": DEMON_FLOPS_PER_LINK,
+                     "peak_source": "measured CUDA-core FP64 FMA throughput / 148 SMs"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * args.steps / wall, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 48 + 8,
+                "path": "mag_demon_microcanonical wall clock (links resident; demon energies and the "
+                        "reunitarisation deviation read back after every sweep)"},
+        "clocks": clocks,
+        "gpu_launches": 4 * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -685,6 +793,8 @@ def main():
     if args.impl == "reference":
         if params.get("kind") == "nersc":
             nersc_reference_arm(args, params, rank, world)
+        elif params.get("kind") == "demon":
+            demon_reference_arm(args, params, rank, world)
         else:
             reference_arm(args, params, rank, world)
         return
@@ -706,6 +816,8 @@ def main():
     try:
         if params.get("kind") == "nersc":
             run_nersc(args, params, rank, world, dist)
+        elif params.get("kind") == "demon":
+            run_demon(args, params, rank, world, dist)
         else:
             run_gpu(args, params, rank, world, dist)
     finally:

@@ -166,9 +166,10 @@ struct DemonState {
 };
 // path table [4 mu][kDemonPaths][5] (0-3 forward, 4-7 backward, -1 padding)
 void build_demon_paths(int8_t* out);
-// one sweep over the links of one chain (a single CTA, links in site order)
-void launch_demon_sweep(const ChainInfo& ci, LinkPlanes<double> U, const int8_t* paths, unsigned long long seed,
-                        int sweep, double e_max, DemonState* st, cudaStream_t s);
+// one sweep over the links of one chain (a single CTA, links in site order), on the chain's
+// links in the host AoS layout double[V][4][3][3][2] (16-byte aligned)
+void launch_demon_sweep(const ChainInfo& ci, double* aos, const int8_t* paths, unsigned long long seed, int sweep,
+                        double e_max, DemonState* st, cudaStream_t s);
 
 // ---- measurements (kernels_wloop.cu)
 // planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;

@@ -26,23 +26,54 @@ enum { RNG_DEMON_SU2 = 4, RNG_DEMON_SUBGROUP = 5 };
 
 __device__ __forceinline__ int wrap(int v, int L) { return v < 0 ? v + L : (v >= L ? v - L : v); }
 
+// The sweep works on an AoS copy of one chain's links (link (s, mu) = 9 complex at
+// ((4 s + mu) * 9)): a thread that follows a path reads whole links, two 128-byte
+// lines each, which the neighbouring paths and links reuse from L1.
+struct AosLinks {
+    double2* p;
+    __device__ mat3<double> load(int mu, int s) const {
+        const double2* q = p + ((size_t)s * 4 + mu) * 9;
+        mat3<double> m;
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            const double2 v = q[k];
+            m.e[k / 3][k % 3] = mk(v.x, v.y);
+        }
+        return m;
+    }
+    __device__ void store(int mu, int s, const mat3<double>& m) const {
+        double2* q = p + ((size_t)s * 4 + mu) * 9;
+#pragma unroll
+        for (int k = 0; k < 9; k++) q[k] = make_double2(m.e[k / 3][k % 3].re, m.e[k / 3][k % 3].im);
+    }
+};
+
 // get_path_ordered_product (field-matrix.h:102-131) of the path dir[0..n) from
 // site x: forward steps multiply U_d(y) and move, backward steps move and
-// multiply U_d(y)^dag; the first factor is taken as it is (I * U = U exactly)
-__device__ mat3<double> path_product(const LinkPlanes<double>& U, const ChainInfo& ci, const int x[4],
-                                     const int8_t* dir, int n) {
+// multiply U_d(y)^dag; the first factor is taken as it is (I * U = U exactly).
+// All link addresses are formed first so the (up to five) loads are in flight
+// together.
+__device__ mat3<double> path_product(const AosLinks& U, const ChainInfo& ci, const int x[4], const int8_t* dir,
+                                     int n) {
     int y[4] = {x[0], x[1], x[2], x[3]};
-    mat3<double> m;
-    for (int i = 0; i < n; i++) {
+    int g[kSteps], a[kSteps];
+#pragma unroll
+    for (int i = 0; i < kSteps; i++) {
+        if (i >= n) break;
         const int d = dir[i];
-        const int a = d & 3;
-        if (d >= 4) y[a] = wrap(y[a] - 1, ci.L[a]);
-        const int g = ci.off + y[0] + y[1] * ci.stride[1] + y[2] * ci.stride[2] + y[3] * ci.stride[3];
-        const mat3<double> u = U.load(a, g);
-        if (i == 0) m = d < 4 ? u : adj(u);
-        else m = d < 4 ? mul(m, u) : mul_nd(m, u);
-        if (d < 4) y[a] = wrap(y[a] + 1, ci.L[a]);
+        a[i] = d & 3;
+        if (d >= 4) y[a[i]] = wrap(y[a[i]] - 1, ci.L[a[i]]);
+        g[i] = y[0] + y[1] * ci.stride[1] + y[2] * ci.stride[2] + y[3] * ci.stride[3];
+        if (d < 4) y[a[i]] = wrap(y[a[i]] + 1, ci.L[a[i]]);
     }
+    mat3<double> u[kSteps];
+#pragma unroll
+    for (int i = 0; i < kSteps; i++)
+        if (i < n) u[i] = U.load(a[i], g[i]);
+    mat3<double> m = dir[0] < 4 ? u[0] : adj(u[0]);
+#pragma unroll
+    for (int i = 1; i < kSteps; i++)
+        if (i < n) m = dir[i] < 4 ? mul(m, u[i]) : mul_nd(m, u[i]);
     return m;
 }
 
@@ -72,12 +103,13 @@ __device__ mat3<double> random_su3_from_su2(unsigned long long seed, uint32_t li
     return m;
 }
 
-__global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, LinkPlanes<double> U,
+__global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, AosLinks U,
                                                                   const int8_t* paths, unsigned long long seed,
                                                                   int sweep, double e_max, DemonState* st) {
     __shared__ int8_t sp[4 * kPaths * kSteps];
     __shared__ double prod[kPaths][18];
-    __shared__ double S[4][18];
+    __shared__ double part3[3][4][18];  // each staple sum in three partial sums
+    __shared__ double rnd[2][18];       // the two proposals of the current link
     for (int i = threadIdx.x; i < 4 * kPaths * kSteps; i += blockDim.x) sp[i] = paths[i];
     const int t = threadIdx.x, lane = t & 31;
     double E[4];
@@ -96,7 +128,7 @@ __global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, 
             x[2] = r % ci.L[2]; r /= ci.L[2];
             x[3] = r;
         }
-        // 1. the 168 path products of this link
+        // 1. the 168 path products of this link; the last warp draws the two proposals
         if (t < kPaths) {
             const mat3<double> m = path_product(U, ci, x, sp + (mu * kPaths + t) * kSteps, t < 6 ? 3 : kSteps);
 #pragma unroll
@@ -104,34 +136,46 @@ __global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, 
                 prod[t][2 * k] = m.e[k / 3][k % 3].re;
                 prod[t][2 * k + 1] = m.e[k / 3][k % 3].im;
             }
+        } else if (t >= kDemonThreads - 32 && lane < 2) {
+            const mat3<double> m = random_su3_from_su2(seed, (uint32_t)l, (uint32_t)sweep, (uint32_t)lane);
+#pragma unroll
+            for (int k = 0; k < 9; k++) {
+                rnd[lane][2 * k] = m.e[k / 3][k % 3].re;
+                rnd[lane][2 * k + 1] = m.e[k / 3][k % 3].im;
+            }
         }
         __syncthreads();
-        // 2. the four staple sums, each in path order; plaquette and rectangle sums are
-        //    daggered (get_staple_dagger / get_rectangular_dagger), chair and twist are not
-        if (t < 72) {
-            const int cat = t / 18, comp = t % 18;
+        // 2. the four staple sums in three partial sums each (216 threads); plaquette and
+        //    rectangle sums are daggered (get_staple_dagger / get_rectangular_dagger), chair
+        //    and twist are not
+        if (t < 216) {
+            const int third = t / 72, cat = (t % 72) / 18, comp = t % 18;
             const int p0 = cat == 0 ? 0 : cat == 1 ? 6 : cat == 2 ? 24 : 96;
-            const int p1 = cat == 0 ? 6 : cat == 1 ? 24 : cat == 2 ? 96 : 168;
+            const int n = (cat == 0 ? 6 : cat == 1 ? 18 : 72) / 3;
             const int e = comp >> 1, part = comp & 1;
             const int src = cat < 2 ? 2 * ((e % 3) * 3 + e / 3) + part : comp;  // element (j, i) for the dagger
             double a = 0.0;
-            for (int p = p0; p < p1; p++) a += prod[p][src];
-            S[cat][comp] = (cat < 2 && part) ? -a : a;
+            for (int p = p0 + third * n; p < p0 + (third + 1) * n; p++) a += prod[p][src];
+            part3[third][cat][comp] = (cat < 2 && part) ? -a : a;
         }
         __syncthreads();
-        // 3. two hits (warp 0; lane k < 4 owns the action term k)
+        // 3. two hits (warp 0; lane k < 4 owns the action term k): with X_k = v S_k,
+        //    delta_S[k] = -ReTr(m X_k) + ReTr(X_k)  (field-demon.h:75-78, (m v) S_k = m (v S_k))
         if (t < 32) {
-            const int g = ci.off + s;
+            const int g = s;
             mat3<double> v = U.load(mu, g);
             mat3<double> Sk;
             const int kk = lane < 4 ? lane : 0;
 #pragma unroll
-            for (int c = 0; c < 9; c++) Sk.e[c / 3][c % 3] = mk(S[kk][2 * c], S[kk][2 * c + 1]);
+            for (int c = 0; c < 9; c++)
+                Sk.e[c / 3][c % 3] = mk(part3[0][kk][2 * c] + part3[1][kk][2 * c] + part3[2][kk][2 * c],
+                                        part3[0][kk][2 * c + 1] + part3[1][kk][2 * c + 1] + part3[2][kk][2 * c + 1]);
+            mat3<double> X = mul(v, Sk);
             for (int hit = 0; hit < 2; hit++) {
-                const mat3<double> m = random_su3_from_su2(seed, (uint32_t)l, (uint32_t)sweep, (uint32_t)hit);
-                const mat3<double> mv = mul(m, v);
-                // delta_S[k] = -(m v S_k).ReTr() + (v S_k).ReTr()  (field-demon.h:75-78)
-                const double dS = -retr(mul(mv, Sk)) + retr(mul(v, Sk));
+                mat3<double> m;
+#pragma unroll
+                for (int c = 0; c < 9; c++) m.e[c / 3][c % 3] = mk(rnd[hit][2 * c], rnd[hit][2 * c + 1]);
+                const double dS = -retr_mul(m, X) + retr(X);
                 double d[4];
                 bool ok = true;
 #pragma unroll
@@ -140,7 +184,8 @@ __global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, 
                     ok = ok && E[k] - d[k] > -e_max && E[k] - d[k] < e_max;
                 }
                 if (ok) {
-                    v = mv;
+                    v = mul(m, v);
+                    if (hit == 0) X = mul(m, X);
 #pragma unroll
                     for (int k = 0; k < 4; k++) E[k] -= d[k];
                     acc++;
@@ -212,9 +257,10 @@ void build_demon_paths(int8_t* out) {
     }
 }
 
-void launch_demon_sweep(const ChainInfo& ci, LinkPlanes<double> U, const int8_t* paths, unsigned long long seed,
-                        int sweep, double e_max, DemonState* st, cudaStream_t s) {
-    k_demon_sweep<<<1, kDemonThreads, 0, s>>>(ci, U, paths, seed, sweep, e_max, st);
+void launch_demon_sweep(const ChainInfo& ci, double* aos, const int8_t* paths, unsigned long long seed, int sweep,
+                        double e_max, DemonState* st, cudaStream_t s) {
+    k_demon_sweep<<<1, kDemonThreads, 0, s>>>(ci, AosLinks{reinterpret_cast<double2*>(aos)}, paths, seed, sweep,
+                                              e_max, st);
 }
 
 }  // namespace magb

@@ -926,13 +926,18 @@ int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max
         MAG_CUDA(cudaMemcpy(ctx->d_demon_paths, table.data(), table.size(), cudaMemcpyHostToDevice));
     }
     // the reference sweeps a copy of the field (field-demon.h:47-49) and starts the demons at 0 (:44);
-    // the copy lives in the reject backup, which only a trajectory in progress uses
+    // the copy is the chain's links in the AoS staging buffer, mirrored into the reject backup
+    // (which only a trajectory in progress uses) for the reunitarisation after each sweep
+    const ChainInfo& ci = ctx->hc[chain];
     const DemonState zero{{0.0, 0.0, 0.0, 0.0}, 0, 0};
     MAG_CUDA(cudaMemcpyAsync(ctx->d_demon, &zero, sizeof(zero), cudaMemcpyHostToDevice, ctx->stream));
     LinkPlanes<double> work = ctx->Ubak;
     launch_link_copy(ctx->geom, ctx->U, work, ctx->stream);
+    MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int i = 0; i < n_sweeps; i++) {
-        launch_demon_sweep(ctx->hc[chain], work, ctx->d_demon_paths, seed, i, e_max, ctx->d_demon, ctx->stream);
+        launch_links_to_aos(work, ci.off, ci.V, ctx->staging, ctx->stream);
+        launch_demon_sweep(ci, ctx->staging, ctx->d_demon_paths, seed, i, e_max, ctx->d_demon, ctx->stream);
+        launch_aos_to_links(ctx->staging, ci.off, ci.V, work, ctx->vpad, ctx->stream);
         // field-demon.h:111 reunitarizes the swept field after every sweep
         MAG_CUDA(cudaMemsetAsync(ctx->reunit, 0, sizeof(unsigned long long) * ctx->nchain, ctx->stream));
         launch_reunitarize(ctx->geom, work, LinkPlanes<float>{nullptr, 0}, ctx->reunit, ctx->stream);
@@ -953,6 +958,11 @@ int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max
             if (rejected) *rejected = st.reject;
         }
     }
+    MAG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
+    MAG_TRY(ctx->sync("mag_demon_microcanonical"));
+    float ms = 0.f;
+    MAG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    ctx->last_measure_ms = ms;
     if (n_sweeps == 0) {
         if (accepted) *accepted = 0;
         if (rejected) *rejected = 0;
