@@ -26,6 +26,8 @@ def main(argv=None) -> int:
     ap.add_argument("--kernels", nargs="*", default=[])
     ap.add_argument("--no-tune", action="store_true", help="keep the default variants (255-register cap)")
     ap.add_argument("--probe", action="store_true", help="also report the FMA throughput probes")
+    ap.add_argument("--demon", type=int, default=0, metavar="SWEEPS",
+                    help="also run this many per-link demon sweeps (E_max 50) and report their device time")
     ap.add_argument("--nvtx", action="store_true",
                     help="wrap each --kernels timing loop in an NVTX range time_<kernel> (for ncu --nvtx-include)")
     a = ap.parse_args(argv)
@@ -36,6 +38,10 @@ def main(argv=None) -> int:
         if not a.no_tune:
             out["tuned_min_blocks"] = c.autotune(3)
         out["force_eval_ms"] = c.time_force(a.reps)
+        if a.demon:
+            res = c.demon_microcanonical(a.demon, 50.0, seed=1)
+            out["demon_sweep_ms"] = c.last_measure_ms() / a.demon
+            out["demon_accepted"], out["demon_rejected"] = res["accepted"], res["rejected"]
         for k in a.kernels:
             if a.nvtx:
                 import torch
