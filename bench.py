@@ -165,10 +165,12 @@ class ClockSampler:
     def __init__(self, index: str):
         self.index = index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        import tempfile
+
+        fd, self.path = tempfile.mkstemp(prefix="mag_clocks_", suffix=".csv")
+        os.close(fd)
 
     def start(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, f"--query-gpu={self.FIELDS}",
@@ -187,7 +189,10 @@ class ClockSampler:
             self.proc.kill()
         self.f.close()
         rows = []
-        for line in open(self.path):
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        os.remove(self.path)
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 10:
                 continue
