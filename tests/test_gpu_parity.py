@@ -344,3 +344,21 @@ def test_split_ensemble_reproduces_the_single_context():
                     assert rec[t][j]["accept"] == whole[t][i]["accept"]
                 assert np.array_equal(c.get_gauge(j), U_whole[i])
 
+
+@pytest.mark.parametrize("dims,mag,n_stout", [((2, 2, 4, 4), 2, 0), ((2, 4, 2, 6), 2, 1), ((8, 4, 4, 8), 4, 0),
+                                             ((8, 4, 4, 8), 4, 2), ((6, 2, 10, 4), 0, 1)])
+def test_edge_lattices_force_action_and_trajectory(dims, mag, n_stout):
+    """Extents of 2 (rectangles wrap onto themselves), odd multiples, mag = 4 segments and no
+    constraint: force, action and one trajectory against the oracle."""
+    U = O.gen_hot(dims, 13)
+    po = O.make_params(dims, mag=mag, action=1, n_stout=n_stout, rho=0.1, n_steps=4)
+    with M.Chmc(dims, mag=mag, n_stout=n_stout, rho=0.1, n_steps=4, seed=2) as c:
+        c.set_gauge(U)
+        assert maxrel(c.get_force(), O.force(po, U)) < 1e-11
+        p, r, a = c.gauge_action()
+        pa, ra, aa = O.action(po, U)
+        assert abs(p - pa) <= 1e-12 * abs(pa) and abs(r - ra) <= 1e-12 * abs(ra) and abs(a - aa) <= 1e-12 * abs(aa)
+    res = _run_pair(dims, dict(mag=mag, n_stout=n_stout, rho=0.1, n_steps=4), 1, start_seed=13)
+    g, o, du = res[0]
+    assert abs(g["delta_h"] - o["delta_h"]) < 1e-9 and g["accept"] == o["accept"] and du < 1e-10
+
