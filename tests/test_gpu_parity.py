@@ -362,3 +362,40 @@ def test_edge_lattices_force_action_and_trajectory(dims, mag, n_stout):
     g, o, du = res[0]
     assert abs(g["delta_h"] - o["delta_h"]) < 1e-9 and g["accept"] == o["accept"] and du < 1e-10
 
+
+@pytest.mark.parametrize("n_stout,mag,pair", [(3, 0, False), (3, 2, True), (1, 2, False)])
+def test_gpu_force_is_minus_gpu_action_derivative(n_stout, mag, pair):
+    """The stout chain rule on the GPU against a central finite difference of the GPU's own
+    smeared action: -Re Tr(X F(x,mu)) = dS/deps for U(x,mu) -> exp(i eps X) U(x,mu), or for a
+    constrained pair U(x,mu) -> U(x,mu) exp(-i eps X), U(x+mu,mu) -> exp(i eps X) U(x+mu,mu)."""
+    dims = (4, 4, 4, 6)
+    U = O.gen_hot(dims, 21)
+    rng = np.random.default_rng(5)
+    X = rng.normal(size=(3, 3)) + 1j * rng.normal(size=(3, 3))
+    X = X + X.conj().T
+    X -= np.trace(X) / 3 * np.eye(3)
+    # a pair: (0,0,0,0) along mu = 1, the first link of its mag = 2 segment, and (0,1,0,0);
+    # a single link: (1,0,0,0) along mu = 1, a free link (x0 odd)
+    mu = 1
+    site = 0 if pair else 1
+    nxt = dims[0]
+    with M.Chmc(dims, mag=mag, n_stout=n_stout, rho=0.1) as c:
+        c.set_gauge(U)
+        F = c.get_force()
+
+        def S(eps):
+            V = U.copy()
+            if pair:
+                V[site, mu] = V[site, mu] @ O.expiQ(-X * eps)
+                V[nxt, mu] = O.expiQ(X * eps) @ V[nxt, mu]
+            else:
+                V[site, mu] = O.expiQ(X * eps) @ V[site, mu]
+            c.set_gauge(V)
+            return c.gauge_action()[2]
+
+        h = 1e-5
+        fd = (S(h) - S(-h)) / (2 * h)
+    # the pair moves along the segment; its derivative is the force of the segment's first link
+    an = -np.trace(X @ F[site, mu]).real
+    assert abs(fd - an) < 2e-7 * max(1.0, abs(an)), (fd, an)
+
