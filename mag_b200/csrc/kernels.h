@@ -159,16 +159,27 @@ void launch_payload_to_links(const double* payload, int two_row, int off, int V,
 void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s);
 
 // ---- per-link demon sweep (kernels_demon.cu)
-constexpr int kDemonPaths = 168;  // staple paths per link: 6 plaquette, 18 rectangle, 72 chair, 72 twist
+constexpr int kDemonPaths = 168;   // staple paths per link: 6 plaquette, 18 rectangle, 72 chair, 72 twist
+constexpr int kDemonWindow = 384;  // capacity of the per-site link window (353 used)
 struct DemonState {
     double E[4];  // plaquette, rectangle, chair, twist demons
     long long accept, reject;
 };
-// path table [4 mu][kDemonPaths][5] (0-3 forward, 4-7 backward, -1 padding)
-void build_demon_paths(int8_t* out);
+// The staple paths of the four links of a site as steps through a window of links around the
+// site: packed[n] = site offset of slot n (4 bits per coordinate, biased by 4) | direction << 16
+// (direction 4: the unit matrix that pads the three-link plaquette paths); step i of path p of
+// the link in direction mu reads slot[mu][p][i], as the link (fwd = 1) or its adjoint (fwd = 0)
+struct DemonTables {
+    int nslot;
+    int packed[kDemonWindow];
+    uint16_t slot[4][kDemonPaths][5];
+    uint8_t fwd[4][kDemonPaths][5];
+};
+// false if the path set does not fit the window (cannot happen for the fixed path set)
+bool build_demon_tables(DemonTables* out);
 // one sweep over the links of one chain (a single CTA, links in site order), on the chain's
 // links in the host AoS layout double[V][4][3][3][2] (16-byte aligned)
-void launch_demon_sweep(const ChainInfo& ci, double* aos, const int8_t* paths, unsigned long long seed, int sweep,
+void launch_demon_sweep(const ChainInfo& ci, double* aos, const DemonTables* tabs, unsigned long long seed, int sweep,
                         double e_max, DemonState* st, cudaStream_t s);
 
 // ---- measurements (kernels_wloop.cu)

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <memory>
 #include <vector>
 
 #include "../../include/mag_c.h"
@@ -120,7 +121,7 @@ struct mag_ctx {
     long max_v = 0;
     // NERSC I/O: pinned double buffer, CRC segment registers, word checksum
     nersc::Pinned pin;
-    int8_t* d_demon_paths = nullptr;  // per-link demon sweep: staple path table
+    DemonTables* d_demon_tables = nullptr;  // per-link demon sweep: staple paths through the site window
     DemonState* d_demon = nullptr;
     uint32_t* d_crc = nullptr;      // segment registers (kCrcThreads + 1)
     uint32_t* d_crc2 = nullptr;     // folded groups
@@ -918,12 +919,12 @@ int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max
                              double* reunit) {
     if (!ctx || n_sweeps < 0 || !(e_max >= 0.0)) return fail(MAG_ERR_ARG, "mag_demon_microcanonical: bad argument");
     MAG_TRY(ctx->chain_ok(chain));
-    if (!ctx->d_demon_paths) {
-        std::vector<int8_t> table((size_t)4 * kDemonPaths * 5);
-        build_demon_paths(table.data());
-        MAG_TRY(ctx->alloc((void**)&ctx->d_demon_paths, table.size()));
+    if (!ctx->d_demon_tables) {
+        std::unique_ptr<DemonTables> tabs(new DemonTables);
+        if (!build_demon_tables(tabs.get())) return fail(MAG_ERR_ARG, "demon path window overflow");
+        MAG_TRY(ctx->alloc((void**)&ctx->d_demon_tables, sizeof(DemonTables)));
         MAG_TRY(ctx->alloc((void**)&ctx->d_demon, sizeof(DemonState)));
-        MAG_CUDA(cudaMemcpy(ctx->d_demon_paths, table.data(), table.size(), cudaMemcpyHostToDevice));
+        MAG_CUDA(cudaMemcpy(ctx->d_demon_tables, tabs.get(), sizeof(DemonTables), cudaMemcpyHostToDevice));
     }
     // the reference sweeps a copy of the field (field-demon.h:47-49) and starts the demons at 0 (:44);
     // the copy is the chain's links in the AoS staging buffer, mirrored into the reject backup
@@ -936,7 +937,7 @@ int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max
     MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
     for (int i = 0; i < n_sweeps; i++) {
         launch_links_to_aos(work, ci.off, ci.V, ctx->staging, ctx->stream);
-        launch_demon_sweep(ci, ctx->staging, ctx->d_demon_paths, seed, i, e_max, ctx->d_demon, ctx->stream);
+        launch_demon_sweep(ci, ctx->staging, ctx->d_demon_tables, seed, i, e_max, ctx->d_demon, ctx->stream);
         launch_aos_to_links(ctx->staging, ci.off, ci.V, work, ctx->vpad, ctx->stream);
         // field-demon.h:111 reunitarizes the swept field after every sweep
         MAG_CUDA(cudaMemsetAsync(ctx->reunit, 0, sizeof(unsigned long long) * ctx->nchain, ctx->stream));
