@@ -11,7 +11,12 @@ that a change of the oracle or of the GPU path against them shows up:
   sums, and one constrained force-gradient trajectory (8 steps, mag = 2,
   Metropolis) from given momenta and uniform;
 * ``unit_2x2x2x4.nersc`` / ``hot_2x2x2x4.nersc``: NERSC files (3x3 and two-row)
-  written by the oracle with a fixed ARCHIVE_DATE.
+  written by the oracle with a fixed ARCHIVE_DATE;
+* ``demon_4x4x4x4.npz``: two per-link demon sweeps (E_max = 50, seed 9) of a Haar hot
+  start (seed 5): the demon energies after each sweep, the accepted / rejected hit counts,
+  the reunitarisation deviations and every 7th site of the swept links.
+
+    python tests/golden/make_golden.py --only demon    # one fixture
 """
 from __future__ import annotations
 
@@ -29,11 +34,28 @@ NERSC_DIMS = (2, 2, 2, 4)
 ARCHIVE_TIME = 1735689600  # 2025-01-01 00:00:00 UTC
 
 
-def main() -> None:
+DEMON_SEED, DEMON_SWEEPS, DEMON_EMAX, DEMON_HOT = 9, 2, 50.0, 5
+
+
+def write_demon() -> None:
+    import oracle as O
+
+    U0 = O.gen_hot(DIMS, DEMON_HOT)
+    U1, E, acc, rej, dev = O.demon_sweeps(DIMS, U0, seed=DEMON_SEED, n_sweeps=DEMON_SWEEPS, e_max=DEMON_EMAX)
+    np.savez_compressed(os.path.join(HERE, "demon_4x4x4x4.npz"), E=E, accepted=acc, rejected=rej, reunit=dev,
+                        U_after_every7=U1[::7])
+
+
+def main(only=None) -> None:
     import oracle as O
     from oracle import nersc as N
 
     O.build()
+    if only == "demon":
+        write_demon()
+        print("written to", HERE)
+        return
+    write_demon()
     U = O.gen_hot(DIMS, 3)
     p_thin = O.make_params(DIMS, mag=2, action=1, beta=2.25, n_stout=0, n_steps=8)
     p_st = O.make_params(DIMS, mag=2, action=1, beta=2.25, n_stout=3, rho=0.1, n_steps=8)
@@ -55,4 +77,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[2] if len(sys.argv) > 2 and sys.argv[1] == "--only" else None)

@@ -31,6 +31,22 @@ def test_demon_sweeps_match_oracle(dims, e_max):
     assert np.all(res["reunit_maxdev"] < 1e-13) and np.all(devo < 1e-13)
 
 
+def test_demon_full_sweep_8x8x8x8():
+    """One sweep of all 16384 links of an 8^4 lattice: the site windows are staged over 4096
+    site transitions, with periodic wrap-around in every direction."""
+    dims = (8, 8, 8, 8)
+    U = O.gen_hot(dims, 7)
+    Uo, Eo, ao, ro, devo = O.demon_sweeps(dims, U, seed=21, n_sweeps=1, e_max=50.0)
+    with M.Chmc(dims, mag=0) as c:
+        c.set_gauge(U)
+        res = c.demon_microcanonical(1, 50.0, seed=21, update_links=True)
+        Ug = c.get_gauge()
+    assert res["accepted"] == ao and res["rejected"] == ro
+    assert ao + ro == 2 * 4 * 8 ** 4
+    assert np.abs(res["demon_energy"] - Eo).max() < 1e-9
+    assert np.abs(Ug - Uo).max() < 1e-12
+
+
 def test_demon_sweep_keeps_links_by_default_and_serves_any_chain():
     chains = [dict(dims=(4, 4, 4, 4)), dict(dims=(4, 4, 6, 4))]
     U1 = O.gen_hot((4, 4, 6, 4), 6)

@@ -3,7 +3,8 @@ the FP64 oracle; the reference has no golden vectors of its own).
 
 CPU: the oracle still reproduces them.  GPU: the library matches them to the
 parity bars (force 1e-11 relative, sums 1e-12 relative, Delta H 1e-9, same
-accept, NERSC files load with their header checksum and plaquette).
+accept, NERSC files load with their header checksum and plaquette, demon sweeps
+with the same hit counts and energies within 1e-9).
 """
 import os
 
@@ -64,6 +65,34 @@ def test_nersc_fixtures_oracle_and_header_reader(tmp_path, name, two_row):
         pa = np.frombuffer(open(path, "rb").read()[h["payload_offset"]:], ">f8")
         pb = np.frombuffer(open(out, "rb").read()[read_nersc_header(out)["payload_offset"]:], ">f8")
         assert pa.shape == pb.shape and np.abs(pa - pb).max() < 1e-15
+
+
+DEMON_DIMS, DEMON_HOT, DEMON_SEED, DEMON_SWEEPS, DEMON_EMAX = (4, 4, 4, 4), 5, 9, 2, 50.0
+
+
+@pytest.fixture(scope="module")
+def gd():
+    return dict(np.load(os.path.join(HERE, "demon_4x4x4x4.npz")))
+
+
+def test_oracle_reproduces_demon_fixture(gd):
+    U1, E, acc, rej, dev = O.demon_sweeps(DEMON_DIMS, O.gen_hot(DEMON_DIMS, DEMON_HOT), seed=DEMON_SEED,
+                                          n_sweeps=DEMON_SWEEPS, e_max=DEMON_EMAX)
+    assert acc == int(gd["accepted"]) and rej == int(gd["rejected"])
+    assert np.abs(E - gd["E"]).max() < 1e-12
+    assert np.abs(U1[::7] - gd["U_after_every7"]).max() < 1e-14
+    assert np.all(dev < 1e-13)
+
+
+@pytest.mark.gpu
+def test_gpu_matches_demon_fixture(gd):
+    with M.Chmc(DEMON_DIMS, mag=0) as c:
+        c.set_gauge(O.gen_hot(DEMON_DIMS, DEMON_HOT))
+        res = c.demon_microcanonical(DEMON_SWEEPS, DEMON_EMAX, seed=DEMON_SEED, update_links=True)
+        Ug = c.get_gauge()
+    assert res["accepted"] == int(gd["accepted"]) and res["rejected"] == int(gd["rejected"])
+    assert np.abs(res["demon_energy"] - gd["E"]).max() < 1e-9
+    assert np.abs(Ug[::7] - gd["U_after_every7"]).max() < 1e-12
 
 
 @pytest.mark.gpu
