@@ -69,6 +69,10 @@ WORKLOADS = {
     # a step is one sweep over the 16384 links (sequential by definition)
     "demon_8x8x8x8": dict(dims=(8, 8, 8, 8), beta=2.25, n_stout=0, n_steps=1, precision="fp64", kind="demon",
                           e_max=50.0),
+    # the same sweeps for 148 independent 8^4 chains at once (mag_demon_microcanonical_all, one CTA per chain,
+    # one chain per SM); a step is one sweep of every chain
+    "demon_ensemble_148x8x8x8x8": dict(dims=(8, 8, 8, 8), nchains=148, beta=2.25, n_stout=0, n_steps=1,
+                                       precision="fp64", kind="demon_ensemble", e_max=50.0),
 }
 DEFAULT = "16x16x16x32_iwasaki_3stout"
 COMMON = dict(mag=2, action="iwasaki", c1=-0.331, rho=0.1, tau=1.0, accept="metropolis", integrator="fg")
@@ -724,6 +728,115 @@ def demon_reference_arm(args, params, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+DEMON_ENS_METRIC = "per-link demon link updates/s over an ensemble of chains (one CTA per chain)"
+
+
+def demon_ensemble_config(args, params, world):
+    return {"workload": args.workload, "lattice": "x".join(str(d) for d in params["dims"]),
+            "chains": params["nchains"], "e_max": params["e_max"], "hits_per_link": 2,
+            "demons": "plaquette, rectangle, chair, twist", "parallelism": f"chains x replicas{world}",
+            "l2": "148 x 8^4 links (0.7 GB) exceed the 126 MB L2"}
+
+
+def oracle_ensemble_rate(params, n_chains: int, seed: int):
+    """Link updates/s of the oracle sweeping n_chains chains on all host threads, one chain per
+    thread (the oracle's sweep releases the interpreter lock)."""
+    import concurrent.futures as cf
+
+    import oracle as O
+
+    dims = params["dims"]
+    threads = os.cpu_count() or 1
+    fields = [O.gen_hot(dims, seed + k) for k in range(n_chains)]
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(lambda k: O.demon_sweeps(dims, fields[k], seed + k, 1, params["e_max"]), range(n_chains)))
+    t = time.perf_counter() - t0
+    return n_chains * 4 * site_count(dims) / t, threads, t
+
+
+def demon_ensemble_reference_arm(args, params, rank: int, world: int):
+    """The oracle's sweeps of independent chains on all host threads; a step sweeps one chain per thread."""
+    if rank != 0:
+        return
+    n = os.cpu_count() or 1
+    for i in range(args.warmup):
+        oracle_ensemble_rate(params, 1, 100 + i)
+    rates = [oracle_ensemble_rate(params, n, 1 + n * i)[0] for i in range(args.steps)]
+    rate = statistics.median(rates)
+    step_s = n * 4 * site_count(params["dims"]) / rate
+    line = {"metric": DEMON_ENS_METRIC, "value": rate, "unit": "link updates/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: Philox Haar hot starts", "config": demon_ensemble_config(args, params, world),
+            "cpu_baseline": {"value": rate, "unit": "link updates/s", "cores": n, "kind": "port",
+                             "sample": f"{n} chains swept once per step, one host thread each"},
+            "e2e": {"value": rate, "unit": "link updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_demon_ensemble(args, params, rank, world, dist):
+    import torch
+
+    import mag_b200 as M
+    from mag_b200.field_hmc import probe_fma_peak
+
+    dims, n = params["dims"], params["nchains"]
+    V = site_count(dims)
+    seed = rank_seed(rank)
+    with M.Chmc(chains=[dict(dims=dims, beta=params["beta"], mag=0) for _ in range(n)], n_stout=0, seed=seed) as c:
+        c.hot_start(seed)
+        c.demon_microcanonical_all(args.warmup, params["e_max"], seed=seed)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        sampler = ClockSampler(gpu_index_for_smi()) if rank == 0 else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = c.demon_microcanonical_all(args.steps, params["e_max"], seed=seed + 1)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        dev_s = c.last_measure_ms() / 1e3  # CUDA events on the library's stream around the sweeps
+        clocks = sampler.stop() if sampler else None
+    el = max_over_ranks(dev_s, dist, "cuda")
+    wall = max_over_ranks(wall, dist, "cuda")
+    if rank != 0:
+        return
+    sweep_s = el / args.steps
+    links = world * n * 4 * V
+    flops = DEMON_FLOPS_PER_LINK * links / world / sweep_s / 1e12
+    peak = probe_fma_peak("fp64")
+    cpu = None
+    if not args.no_cpu:
+        rate, threads, tc = oracle_ensemble_rate(params, 2 * (os.cpu_count() or 1), 1)
+        cpu = {"value": rate, "unit": "link updates/s", "cores": threads, "kind": "port",
+               "sample": f"{2 * threads} chains of {'x'.join(map(str, dims))} swept once, one host thread each "
+                         f"({tc:.1f} s)"}
+    line = {
+        "metric": DEMON_ENS_METRIC, "value": links / sweep_s, "unit": "link updates/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sweep_s * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot starts",
+        "config": demon_ensemble_config(args, params, world),
+        "chain_sweeps_per_s": world * n / sweep_s,
+        "accepted": int(sum(r["accepted"] for r in res)), "rejected": int(sum(r["rejected"] for r in res)),
+        "roofline": {"bound": "fp64 (one CTA per chain, sequential inside a chain)", "achieved": flops,
+                     "peak": peak, "unit": "TFLOP/s", "frac": flops / peak, "traffic": None,
+                     "flops_per_link": DEMON_FLOPS_PER_LINK,
+                     "peak_source": "measured CUDA-core FP64 FMA throughput of the device"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * n * 4 * V * args.steps / wall, "unit": "link updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": n * (48 + 8),
+                "path": "mag_demon_microcanonical_all wall clock (links resident; every chain's demon energies "
+                        "and reunitarisation deviation read back after every sweep)"},
+        "clocks": clocks,
+        "gpu_launches": (2 * n + 2) * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_demon(args, params, rank, world, dist):
     import torch
 
@@ -800,6 +913,8 @@ def main():
             nersc_reference_arm(args, params, rank, world)
         elif params.get("kind") == "demon":
             demon_reference_arm(args, params, rank, world)
+        elif params.get("kind") == "demon_ensemble":
+            demon_ensemble_reference_arm(args, params, rank, world)
         else:
             reference_arm(args, params, rank, world)
         return
@@ -823,6 +938,8 @@ def main():
             run_nersc(args, params, rank, world, dist)
         elif params.get("kind") == "demon":
             run_demon(args, params, rank, world, dist)
+        elif params.get("kind") == "demon_ensemble":
+            run_demon_ensemble(args, params, rank, world, dist)
         else:
             run_gpu(args, params, rank, world, dist)
     finally:

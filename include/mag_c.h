@@ -183,6 +183,14 @@ int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);
 int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max, uint64_t seed,
                              int update_links, double* demon_energy, int64_t* accepted, int64_t* rejected,
                              double* reunit);
+/* The same sweeps for every chain of an ensemble context at once, one CTA per chain
+   (no reference counterpart: the reference sweeps one field).  Chain c draws with the
+   Philox key seed + its stream index (the chain's index unless mag_set_stream_index
+   changed it), so its result equals mag_demon_microcanonical(ctx, c, ..., seed + index).
+   demon_energy[(c * n_sweeps + i) * 4 + k], reunit[c * n_sweeps + i], accepted[c],
+   rejected[c] (any may be NULL). */
+int mag_demon_microcanonical_all(mag_ctx* ctx, int n_sweeps, double e_max, uint64_t seed, int update_links,
+                                 double* demon_energy, int64_t* accepted, int64_t* rejected, double* reunit);
 
 /* ------------------------------------------------------------ measurement */
 /* avg_wilson_loop (field-wloop.h:58-99) for a general spatial vector r and extent T */

@@ -177,10 +177,17 @@ struct DemonTables {
 };
 // false if the path set does not fit the window (cannot happen for the fixed path set)
 bool build_demon_tables(DemonTables* out);
-// one sweep over the links of one chain (a single CTA, links in site order), on the chain's
-// links in the host AoS layout double[V][4][3][3][2] (16-byte aligned)
-void launch_demon_sweep(const ChainInfo& ci, double* aos, const DemonTables* tabs, unsigned long long seed, int sweep,
-                        double e_max, DemonState* st, cudaStream_t s);
+// One sweep of one chain: its links in the host AoS layout double[V][4][3][3][2] start at
+// double2 aos_off of the AoS buffer; its Philox draws use the key `seed`.
+struct DemonJob {
+    ChainInfo ci;
+    long long aos_off;
+    unsigned long long seed;
+};
+// one sweep of each of njobs chains, one CTA per chain (links in site order inside a chain,
+// the chains side by side); states[j] holds chain j's demons and hit counts
+void launch_demon_sweeps(const DemonJob* jobs, int njobs, double* aos, const DemonTables* tabs, int sweep,
+                         double e_max, DemonState* states, cudaStream_t s);
 
 // ---- measurements (kernels_wloop.cu)
 // planar R x T loops: lines = Rmax single-direction planes, tl/tl2 = two more;

@@ -4,7 +4,8 @@
 // The reference updates the links one after another in site-index order
 // (x0 fastest, mu = 0..3 inner), each update seeing every earlier one, and four
 // global demons decide every hit: the sweep is sequential by definition.  One
-// CTA walks the links in that order and parallelises inside a link:
+// CTA walks the links of one chain in that order (independent chains of an
+// ensemble run side by side, one CTA each) and parallelises inside a link:
 //
 //  * window: the 353 distinct links that the 168 staple paths of the four links
 //    of a site touch are staged in shared memory, one window per site, with
@@ -159,9 +160,13 @@ __device__ __forceinline__ mat3<double> load_oriented(const double2* q, bool fwd
     return o;
 }
 
-__global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(ChainInfo ci, double2* U, const DemonTables* tabs,
-                                                                  unsigned long long seed, int sweep, double e_max,
-                                                                  DemonState* st) {
+__global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(const DemonJob* jobs, double2* aos,
+                                                                  const DemonTables* tabs, int sweep, double e_max,
+                                                                  DemonState* states) {
+    const ChainInfo ci = jobs[blockIdx.x].ci;
+    double2* U = aos + jobs[blockIdx.x].aos_off;
+    const unsigned long long seed = jobs[blockIdx.x].seed;
+    DemonState* st = states + blockIdx.x;
     extern __shared__ __align__(16) unsigned char dsm[];
     double2* win = reinterpret_cast<double2*>(dsm);  // [2][kDemonWindow][9]: windows of sites s, s + 1
     double(*prod)[18] = reinterpret_cast<double(*)[18]>(dsm + 2 * kDemonWindow * kLinkBytes);  // [kPaths][18]
@@ -469,11 +474,11 @@ bool build_demon_tables(DemonTables* T) {
     return true;
 }
 
-void launch_demon_sweep(const ChainInfo& ci, double* aos, const DemonTables* tabs, unsigned long long seed, int sweep,
-                        double e_max, DemonState* st, cudaStream_t s) {
+void launch_demon_sweeps(const DemonJob* jobs, int njobs, double* aos, const DemonTables* tabs, int sweep,
+                         double e_max, DemonState* states, cudaStream_t s) {
     cudaFuncSetAttribute(k_demon_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDemonDynSmem);
-    k_demon_sweep<<<1, kDemonThreads, kDemonDynSmem, s>>>(ci, reinterpret_cast<double2*>(aos), tabs, seed, sweep,
-                                                           e_max, st);
+    k_demon_sweep<<<(unsigned)njobs, kDemonThreads, kDemonDynSmem, s>>>(jobs, reinterpret_cast<double2*>(aos), tabs,
+                                                                        sweep, e_max, states);
 }
 
 }  // namespace magb

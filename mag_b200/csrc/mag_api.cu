@@ -122,7 +122,10 @@ struct mag_ctx {
     // NERSC I/O: pinned double buffer, CRC segment registers, word checksum
     nersc::Pinned pin;
     DemonTables* d_demon_tables = nullptr;  // per-link demon sweep: staple paths through the site window
-    DemonState* d_demon = nullptr;
+    DemonState* d_demon = nullptr;          // one per chain
+    DemonJob* d_demon_jobs = nullptr;       // one per chain
+    double* demon_aos = nullptr;            // AoS copy of every chain (sweeps of the whole ensemble)
+    std::vector<unsigned long long> h_stream_index;
     uint32_t* d_crc = nullptr;      // segment registers (kCrcThreads + 1)
     uint32_t* d_crc2 = nullptr;     // folded groups
     uint32_t* d_crc_tab = nullptr;  // 4 x 256 shift tables of one segment
@@ -249,6 +252,7 @@ struct mag_ctx {
         std::vector<unsigned long long> sidx(n);
         for (int c = 0; c < n; c++) sidx[c] = (unsigned long long)c;
         MAG_CUDA(cudaMemcpy(d_stream_index, sidx.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice));
+        h_stream_index = sidx;
         geom = DevGeom{d_chains, d_c2c, vpad, n, d_stream_index};
 
         MAG_TRY(alloc_links(U));
@@ -914,49 +918,75 @@ int mag_trajectory(mag_ctx* ctx, int refresh, mag_traj_result* results) {
     return MAG_OK;
 }
 
-int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max, uint64_t seed,
-                             int update_links, double* demon_energy, int64_t* accepted, int64_t* rejected,
-                             double* reunit) {
-    if (!ctx || n_sweeps < 0 || !(e_max >= 0.0)) return fail(MAG_ERR_ARG, "mag_demon_microcanonical: bad argument");
-    MAG_TRY(ctx->chain_ok(chain));
+namespace {
+
+// n_sweeps demon sweeps of the chains `chains` (all of one context), each on an AoS copy of its
+// links: one CTA per chain and sweep launch.  Outputs per listed chain j: demon_energy[(j *
+// n_sweeps + i) * 4 + k], reunit[j * n_sweeps + i], accepted[j], rejected[j] (any may be NULL).
+int demon_sweeps(mag_ctx* ctx, const std::vector<int>& chains, const std::vector<unsigned long long>& seeds,
+                 int n_sweeps, double e_max, int update_links, double* demon_energy, int64_t* accepted,
+                 int64_t* rejected, double* reunit) {
+    const int nj = (int)chains.size();
     if (!ctx->d_demon_tables) {
         std::unique_ptr<DemonTables> tabs(new DemonTables);
         if (!build_demon_tables(tabs.get())) return fail(MAG_ERR_ARG, "demon path window overflow");
         MAG_TRY(ctx->alloc((void**)&ctx->d_demon_tables, sizeof(DemonTables)));
-        MAG_TRY(ctx->alloc((void**)&ctx->d_demon, sizeof(DemonState)));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_demon, sizeof(DemonState) * ctx->nchain));
+        MAG_TRY(ctx->alloc((void**)&ctx->d_demon_jobs, sizeof(DemonJob) * ctx->nchain));
         MAG_CUDA(cudaMemcpy(ctx->d_demon_tables, tabs.get(), sizeof(DemonTables), cudaMemcpyHostToDevice));
     }
+    // one chain: its AoS copy in the staging buffer; several: the ensemble-wide AoS buffer
+    double* aos = ctx->staging;
+    if (nj > 1) {
+        if (!ctx->demon_aos) MAG_TRY(ctx->alloc((void**)&ctx->demon_aos, sizeof(double) * 72 * (size_t)ctx->vpad));
+        aos = ctx->demon_aos;
+    }
+    std::vector<DemonJob> jobs(nj);
+    for (int j = 0; j < nj; j++) {
+        const ChainInfo& ci = ctx->hc[chains[j]];
+        jobs[j].ci = ci;
+        jobs[j].aos_off = nj > 1 ? 36LL * ci.off : 0;
+        jobs[j].seed = seeds[j];
+    }
     // the reference sweeps a copy of the field (field-demon.h:47-49) and starts the demons at 0 (:44);
-    // the copy is the chain's links in the AoS staging buffer, mirrored into the reject backup
-    // (which only a trajectory in progress uses) for the reunitarisation after each sweep
-    const ChainInfo& ci = ctx->hc[chain];
-    const DemonState zero{{0.0, 0.0, 0.0, 0.0}, 0, 0};
-    MAG_CUDA(cudaMemcpyAsync(ctx->d_demon, &zero, sizeof(zero), cudaMemcpyHostToDevice, ctx->stream));
+    // the copy is kept in the reject backup (which only a trajectory in progress uses) and swept as
+    // AoS links, then converted back for the reunitarisation after each sweep
+    const std::vector<DemonState> zero(nj, DemonState{{0.0, 0.0, 0.0, 0.0}, 0, 0});
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_demon_jobs, jobs.data(), sizeof(DemonJob) * nj, cudaMemcpyHostToDevice,
+                             ctx->stream));
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_demon, zero.data(), sizeof(DemonState) * nj, cudaMemcpyHostToDevice,
+                             ctx->stream));
     LinkPlanes<double> work = ctx->Ubak;
     launch_link_copy(ctx->geom, ctx->U, work, ctx->stream);
     MAG_CUDA(cudaEventRecord(ctx->ev0, ctx->stream));
+    std::vector<DemonState> st(nj);
+    std::vector<unsigned long long> bits(ctx->nchain);
     for (int i = 0; i < n_sweeps; i++) {
-        launch_links_to_aos(work, ci.off, ci.V, ctx->staging, ctx->stream);
-        launch_demon_sweep(ci, ctx->staging, ctx->d_demon_tables, seed, i, e_max, ctx->d_demon, ctx->stream);
-        launch_aos_to_links(ctx->staging, ci.off, ci.V, work, ctx->vpad, ctx->stream);
+        for (int j = 0; j < nj; j++) {
+            const ChainInfo& ci = ctx->hc[chains[j]];
+            launch_links_to_aos(work, ci.off, ci.V, aos + 2 * jobs[j].aos_off, ctx->stream);
+        }
+        launch_demon_sweeps(ctx->d_demon_jobs, nj, aos, ctx->d_demon_tables, i, e_max, ctx->d_demon, ctx->stream);
+        for (int j = 0; j < nj; j++) {
+            const ChainInfo& ci = ctx->hc[chains[j]];
+            launch_aos_to_links(aos + 2 * jobs[j].aos_off, ci.off, ci.V, work, ctx->vpad, ctx->stream);
+        }
         // field-demon.h:111 reunitarizes the swept field after every sweep
         MAG_CUDA(cudaMemsetAsync(ctx->reunit, 0, sizeof(unsigned long long) * ctx->nchain, ctx->stream));
         launch_reunitarize(ctx->geom, work, LinkPlanes<float>{nullptr, 0}, ctx->reunit, ctx->stream);
-        DemonState st;
-        unsigned long long bits = 0;
-        MAG_CUDA(cudaMemcpyAsync(&st, ctx->d_demon, sizeof(st), cudaMemcpyDeviceToHost, ctx->stream));
-        MAG_CUDA(cudaMemcpyAsync(&bits, ctx->reunit + chain, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+        MAG_CUDA(cudaMemcpyAsync(st.data(), ctx->d_demon, sizeof(DemonState) * nj, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        MAG_CUDA(cudaMemcpyAsync(bits.data(), ctx->reunit, sizeof(unsigned long long) * ctx->nchain,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
         MAG_TRY(ctx->sync("mag_demon_microcanonical"));
-        if (demon_energy)
-            for (int k = 0; k < 4; k++) demon_energy[4 * i + k] = st.E[k];
-        if (reunit) {
-            double d;
-            memcpy(&d, &bits, sizeof(d));
-            reunit[i] = d;
-        }
-        if (i == n_sweeps - 1) {
-            if (accepted) *accepted = st.accept;
-            if (rejected) *rejected = st.reject;
+        for (int j = 0; j < nj; j++) {
+            if (demon_energy)
+                for (int k = 0; k < 4; k++) demon_energy[((size_t)j * n_sweeps + i) * 4 + k] = st[j].E[k];
+            if (reunit) {
+                double d;
+                memcpy(&d, &bits[chains[j]], sizeof(d));
+                reunit[(size_t)j * n_sweeps + i] = d;
+            }
         }
     }
     MAG_CUDA(cudaEventRecord(ctx->ev1, ctx->stream));
@@ -964,15 +994,39 @@ int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max
     float ms = 0.f;
     MAG_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
     ctx->last_measure_ms = ms;
-    if (n_sweeps == 0) {
-        if (accepted) *accepted = 0;
-        if (rejected) *rejected = 0;
+    for (int j = 0; j < nj; j++) {
+        if (accepted) accepted[j] = n_sweeps ? st[j].accept : 0;
+        if (rejected) rejected[j] = n_sweeps ? st[j].reject : 0;
     }
     if (update_links) {
         launch_link_copy(ctx->geom, work, ctx->U, ctx->stream);
         MAG_TRY(ctx->refresh_copy());
     }
     return ctx->sync("mag_demon_microcanonical");
+}
+
+}  // namespace
+
+int mag_demon_microcanonical(mag_ctx* ctx, int chain, int n_sweeps, double e_max, uint64_t seed,
+                             int update_links, double* demon_energy, int64_t* accepted, int64_t* rejected,
+                             double* reunit) {
+    if (!ctx || n_sweeps < 0 || !(e_max >= 0.0)) return fail(MAG_ERR_ARG, "mag_demon_microcanonical: bad argument");
+    MAG_TRY(ctx->chain_ok(chain));
+    return demon_sweeps(ctx, {chain}, {(unsigned long long)seed}, n_sweeps, e_max, update_links, demon_energy,
+                        accepted, rejected, reunit);
+}
+
+int mag_demon_microcanonical_all(mag_ctx* ctx, int n_sweeps, double e_max, uint64_t seed, int update_links,
+                                 double* demon_energy, int64_t* accepted, int64_t* rejected, double* reunit) {
+    if (!ctx || n_sweeps < 0 || !(e_max >= 0.0))
+        return fail(MAG_ERR_ARG, "mag_demon_microcanonical_all: bad argument");
+    std::vector<int> chains(ctx->nchain);
+    std::vector<unsigned long long> seeds(ctx->nchain);
+    for (int c = 0; c < ctx->nchain; c++) {
+        chains[c] = c;
+        seeds[c] = (unsigned long long)seed + ctx->h_stream_index[c];
+    }
+    return demon_sweeps(ctx, chains, seeds, n_sweeps, e_max, update_links, demon_energy, accepted, rejected, reunit);
 }
 
 int mag_fg_trajectory(mag_ctx* ctx, int refresh_momenta, mag_traj_result* results) {
@@ -1026,7 +1080,9 @@ int mag_set_stream_index(mag_ctx* ctx, const int64_t* index) {
     }
     MAG_CUDA(cudaMemcpyAsync(ctx->d_stream_index, v.data(), sizeof(unsigned long long) * v.size(),
                              cudaMemcpyHostToDevice, ctx->stream));
-    return ctx->sync("mag_set_stream_index");
+    MAG_TRY(ctx->sync("mag_set_stream_index"));
+    ctx->h_stream_index = v;
+    return MAG_OK;
 }
 
 int mag_traj_counter(mag_ctx* ctx, int64_t* traj) {

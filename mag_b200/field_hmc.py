@@ -279,6 +279,23 @@ class Chmc:
                                                  ctypes.byref(r), _dp(dev)), "mag_demon_microcanonical")
         return {"demon_energy": E, "accepted": a.value, "rejected": r.value, "reunit_maxdev": dev}
 
+    def demon_microcanonical_all(self, n_sweeps: int, e_max: float, seed: int = 1,
+                                 update_links: bool = False) -> list[dict]:
+        """The per-link demon sweeps of every chain at once (one CTA per chain).  Chain c draws
+        with the key seed + its stream index, so entry c equals
+        demon_microcanonical(n_sweeps, e_max, seed + index, chain=c)."""
+        n = self.n_chains
+        E = np.zeros((n, int(n_sweeps), 4))
+        dev = np.zeros((n, int(n_sweeps)))
+        a, r = np.zeros(n, np.int64), np.zeros(n, np.int64)
+        check(self._lib.mag_demon_microcanonical_all(self._h, int(n_sweeps), float(e_max), int(seed),
+                                                     1 if update_links else 0, _dp(E),
+                                                     a.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                     r.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _dp(dev)),
+              "mag_demon_microcanonical_all")
+        return [{"demon_energy": E[c], "accepted": int(a[c]), "rejected": int(r[c]), "reunit_maxdev": dev[c]}
+                for c in range(n)]
+
     # ------------------------------------------------------------ NERSC I/O
     def export_config_nersc(self, path: str, beta: float | None = None, sequence_num: int = 0,
                             ensemble_label: str = "", skip_third: bool = True, chain: int = 0) -> dict:

@@ -60,6 +60,35 @@ def test_demon_sweep_keeps_links_by_default_and_serves_any_chain():
     assert res["accepted"] == ao and np.abs(res["demon_energy"] - Eo).max() < 1e-9
 
 
+def test_ensemble_sweeps_each_chain_like_the_oracle():
+    """mag_demon_microcanonical_all: every chain of an ensemble swept at once, one CTA per
+    chain, chain c drawing with seed + its stream index."""
+    dims = [(4, 4, 4, 4), (4, 4, 4, 6), (2, 4, 2, 4)]
+    hot = [O.gen_hot(d, 11 + c) for c, d in enumerate(dims)]
+    with M.Chmc(chains=[dict(dims=d, mag=0) for d in dims]) as c:
+        c.set_stream_index([5, 6, 7])
+        for k, U in enumerate(hot):
+            c.set_gauge(U, chain=k)
+        res = c.demon_microcanonical_all(2, 30.0, seed=9, update_links=True)
+        Ug = [c.get_gauge(k) for k in range(len(dims))]
+    for k, d in enumerate(dims):
+        Uo, Eo, ao, ro, devo = O.demon_sweeps(d, hot[k], seed=9 + 5 + k, n_sweeps=2, e_max=30.0)
+        assert res[k]["accepted"] == ao and res[k]["rejected"] == ro
+        assert np.abs(res[k]["demon_energy"] - Eo).max() < 1e-9
+        assert np.abs(Ug[k] - Uo).max() < 1e-12
+        assert np.all(res[k]["reunit_maxdev"] < 1e-13)
+
+
+def test_ensemble_sweeps_keep_links_by_default():
+    dims = [(4, 4, 4, 4), (2, 4, 2, 4)]
+    with M.Chmc(chains=[dict(dims=d, mag=0) for d in dims]) as c:
+        c.hot_start(3)
+        U0 = [c.get_gauge(k) for k in range(2)]
+        res = c.demon_microcanonical_all(1, 30.0, seed=2)
+        assert all(np.array_equal(c.get_gauge(k), U0[k]) for k in range(2))
+    assert all(r["accepted"] + r["rejected"] == 2 * 4 * int(np.prod(d)) for r, d in zip(res, dims))
+
+
 def test_zero_window_accepts_nothing():
     U = O.gen_hot((4, 4, 4, 4), 2)
     with M.Chmc((4, 4, 4, 4), mag=0) as c:
