@@ -109,6 +109,20 @@ __device__ __forceinline__ void apply_su2(mat3<double>& v, const Su2& m, bool ap
         }
     }
 }
+// one column of v <- m v (the operations of apply_su2 on that column)
+__device__ __forceinline__ void apply_su2_col(cplx<double> col[3], const Su2& m, bool apply) {
+    const cplx<double> vi = pick(col[0], col[1], col[2], m.i);
+    const cplx<double> vj = pick(col[0], col[1], col[2], m.j);
+    cplx<double> ni = cmul<false, false>(m.ii, vi);
+    cmac<false, false, false>(ni, m.ij, vj);
+    cplx<double> nj = cmul<false, false>(m.ji, vi);
+    cmac<false, false, false>(nj, m.jj, vj);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        if (apply && r == m.i) col[r] = ni;
+        if (apply && r == m.j) col[r] = nj;
+    }
+}
 // ReTr(v S) - ReTr(m v S) (field-demon.h:75-78): only the 2x2 block of X = v S on rows and
 // columns i, j enters, the other diagonal elements of m X and X being equal
 __device__ __forceinline__ double delta_s(const mat3<double>& v, const mat3<double>& S, const Su2& m) {
@@ -360,12 +374,20 @@ __global__ void __launch_bounds__(kDemonThreads, 1) k_demon_sweep(const DemonJob
             } else {
                 rej++;
             }
-            apply_su2(v, m0, ok0);
-            apply_su2(v, m1, ok1);
-            if (lane < 9) {
-                const double2 q = make_double2(v.e[lane / 3][lane % 3].re, v.e[lane / 3][lane % 3].im);
-                sbuf[cs][mu][lane] = q;
-                U[((size_t)s * 4 + mu) * 9 + lane] = q;
+            // the updated link, one element per lane 0..8: column c of v through both decisions
+            {
+                const int e = lane < 9 ? lane : 0, r = e / 3, cc = e % 3;
+                cplx<double> col[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) col[k] = pick(v.e[k][0], v.e[k][1], v.e[k][2], cc);
+                apply_su2_col(col, m0, ok0);
+                apply_su2_col(col, m1, ok1);
+                const cplx<double> o = pick(col[0], col[1], col[2], r);
+                if (lane < 9) {
+                    const double2 q = make_double2(o.re, o.im);
+                    sbuf[cs][mu][lane] = q;
+                    U[((size_t)s * 4 + mu) * 9 + lane] = q;
+                }
             }
         } else if (s + 1 < nsite) {
             stage_site(s + 1, wb ^ 1, mu, 32, kDemonThreads - 32, s);
