@@ -437,46 +437,58 @@ def run_gpu(args, params, rank, world, dist):
                               "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
                                               else "fallback 6.65 TB/s")}
 
-    # end to end through the public API with pinned host buffers (chain 0)
+    # end to end through the public API with pinned host buffers (every chain of this rank's context)
     e2e = None
-    if args.e2e_steps > 0 and nchain == 1:
-        V0 = c64.volume(0)
-        field_bytes = V0 * 4 * 9 * 16
-        Uh = torch.empty(V0 * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(V0, 4,
-                                                                                                            3, 3)
-        c64.get_gauge(out=Uh)
+    if args.e2e_steps > 0:
+        nloc = c64.n_chains
+
+        def pinned_field(V):
+            return torch.empty(V * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(
+                V, 4, 3, 3)
+
+        Uh = [pinned_field(c64.volume(k)) for k in range(nloc)]
+        for k in range(nloc):
+            c64.get_gauge(k, out=Uh[k])
         rng = np.random.default_rng(seed)
-        Ps = []  # pinned momentum fields (two, used in turn), filled before the timed region
         s2, s6 = 1 / np.sqrt(2), 1 / np.sqrt(6)
+        Ps = []  # pinned momentum fields (two sets, used in turn), filled before the timed region
         for _ in range(min(args.e2e_steps, 2)):
-            xi = rng.standard_normal((V0, 4, 8))
-            P = torch.empty(V0 * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(
-                V0, 4, 3, 3)
-            P[..., 0, 1] = (xi[..., 0] - 1j * xi[..., 1]) * s2
-            P[..., 0, 2] = (xi[..., 3] - 1j * xi[..., 4]) * s2
-            P[..., 1, 2] = (xi[..., 5] - 1j * xi[..., 6]) * s2
-            P[..., 1, 0] = P[..., 0, 1].conj()
-            P[..., 2, 0] = P[..., 0, 2].conj()
-            P[..., 2, 1] = P[..., 1, 2].conj()
-            P[..., 0, 0] = xi[..., 2] * s2 + xi[..., 7] * s6
-            P[..., 1, 1] = -xi[..., 2] * s2 + xi[..., 7] * s6
-            P[..., 2, 2] = -2 * xi[..., 7] * s6
-            Ps.append(P)
+            Pset = []
+            for k in range(nloc):
+                V = c64.volume(k)
+                xi = rng.standard_normal((V, 4, 8))
+                P = pinned_field(V)
+                P[..., 0, 1] = (xi[..., 0] - 1j * xi[..., 1]) * s2
+                P[..., 0, 2] = (xi[..., 3] - 1j * xi[..., 4]) * s2
+                P[..., 1, 2] = (xi[..., 5] - 1j * xi[..., 6]) * s2
+                P[..., 1, 0] = P[..., 0, 1].conj()
+                P[..., 2, 0] = P[..., 0, 2].conj()
+                P[..., 2, 1] = P[..., 1, 2].conj()
+                P[..., 0, 0] = xi[..., 2] * s2 + xi[..., 7] * s6
+                P[..., 1, 1] = -xi[..., 2] * s2 + xi[..., 7] * s6
+                P[..., 2, 2] = -2 * xi[..., 7] * s6
+                Pset.append(P)
+            Ps.append(Pset)
+        field_bytes = sum(c64.volume(k) for k in range(nloc)) * 4 * 9 * 16
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for k in range(args.e2e_steps):
-            c64.set_gauge(Uh)
-            c64.init_momentum(Ps[k % len(Ps)])
-            c64.set_uniforms([0.5])
+        for j in range(args.e2e_steps):
+            for k in range(nloc):
+                c64.set_gauge(Uh[k], chain=k)
+                c64.init_momentum(Ps[j % len(Ps)][k], chain=k)
+            c64.set_uniforms([0.5] * nloc)
             c64.trajectory(refresh_momenta=False)
             if wl:
                 c64.wilson_loops(wl, wl)
-            c64.get_gauge(out=Uh)
+            for k in range(nloc):
+                c64.get_gauge(k, out=Uh[k])
         torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t0, dist, "cuda")
-        e2e = {"value": world * args.e2e_steps / el, "unit": "traj/s", "h2d_bytes_per_step": 2 * field_bytes + 8,
-               "d2h_bytes_per_step": field_bytes + 152, "steps": args.e2e_steps,
-               "path": "mag_gauge_set + mag_momentum_set + mag_uniforms_set + mag_trajectory + mag_gauge_get"}
+        e2e = {"value": job_chains * args.e2e_steps / el, "unit": "traj/s",
+               "h2d_bytes_per_step": 2 * field_bytes + 8 * nloc, "d2h_bytes_per_step": field_bytes + 152 * nloc,
+               "steps": args.e2e_steps,
+               "path": "mag_gauge_set + mag_momentum_set per chain, mag_uniforms_set, mag_trajectory, "
+                       "mag_gauge_get per chain"}
     c64.close()
 
     mixed = None
