@@ -3,8 +3,8 @@
     python -m mag_b200.profile_driver --dims 24 24 24 24 --n-stout 3 --precision fp64 --reps 2
 
 Creates one context, draws a Philox hot start, then times `reps` force
-evaluations (plus one warm-up evaluation) and the named single kernels, and
-prints the CUDA-event times.  Every launch uses live data, so a profiler that
+evaluations (plus one warm-up evaluation), optionally `--traj` whole
+trajectories, and the named single kernels, and prints the CUDA-event times.  Every launch uses live data, so a profiler that
 selects any of them sees a representative kernel.
 """
 from __future__ import annotations
@@ -30,8 +30,12 @@ def main(argv=None) -> int:
                     help="also run this many per-link demon sweeps (E_max 50) and report their device time")
     ap.add_argument("--nvtx", action="store_true",
                     help="wrap each --kernels timing loop in an NVTX range time_<kernel> (for ncu --nvtx-include)")
+    ap.add_argument("--n-steps", type=int, default=12, help="force-gradient steps per trajectory")
+    ap.add_argument("--traj", type=int, default=0,
+                    help="also run this many trajectories after one warm-up trajectory (inside an NVTX range "
+                         "'trajectories' with --nvtx) and report their device time")
     a = ap.parse_args(argv)
-    with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1,
+    with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1, n_steps=a.n_steps,
                 precision=a.precision, seed=1) as c:
         c.hot_start(1)
         out = {"dims": a.dims, "precision": a.precision, "n_stout": a.n_stout}
@@ -42,6 +46,19 @@ def main(argv=None) -> int:
             res = c.demon_microcanonical(a.demon, 50.0, seed=1)
             out["demon_sweep_ms"] = c.last_measure_ms() / a.demon
             out["demon_accepted"], out["demon_rejected"] = res["accepted"], res["rejected"]
+        if a.traj:
+            import torch
+
+            c.run_chmc(1)
+            torch.cuda.synchronize()
+            if a.nvtx:
+                torch.cuda.nvtx.range_push("trajectories")
+            recs = c.run_chmc(a.traj)
+            torch.cuda.synchronize()
+            if a.nvtx:
+                torch.cuda.nvtx.range_pop()
+            out["traj_ms"] = c.last_run_ms() / a.traj
+            out["delta_h"] = [r[0]["delta_h"] for r in recs]
         for k in a.kernels:
             if a.nvtx:
                 import torch
