@@ -120,7 +120,8 @@ def _run_pair(dims, kw, n_traj, seed=31, start_seed=4):
                        beta=kw.get("beta", 2.25), n_stout=kw.get("n_stout", 0), rho=kw.get("rho", 0.1),
                        n_steps=kw.get("n_steps", 8), tau=kw.get("tau", 1.0),
                        accept=1 if kw.get("accept", "metropolis") == "demon" else 0, e_max=kw.get("e_max", 100.0),
-                       integrator=1 if kw.get("integrator", "fg") == "leapfrog" else 0)
+                       integrator=1 if kw.get("integrator", "fg") == "leapfrog" else 0,
+                       n_forced=kw.get("n_forced_accept", 0))
     U = O.gen_hot(dims, start_seed)
     Uo = U.copy()
     demon = [0.0, 0.0]
@@ -147,6 +148,19 @@ def test_trajectory_parity_8x4_iwasaki_fp64_metropolis():
         assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
         assert g["accept"] == o["accept"]
         assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-12
+        assert du < 1e-10
+
+
+def test_forced_accepts_then_metropolis():
+    """num_forced_accept_step (field-hmc.h:826): the first trajectories are accepted whatever
+    Delta H; with 2 coarse steps trajectory 1 has Delta H ~ 1e2 and is kept only because it is
+    forced, trajectories 2 and 3 fall back to Metropolis."""
+    res = _run_pair((4, 4, 4, 4), dict(mag=2, n_steps=2, n_forced_accept=2), 4)
+    assert [g["accept"] for g, _, _ in res][:2] == [1, 1]
+    assert res[1][1]["delta_h"] > 10.0
+    for g, o, du in res:
+        assert g["accept"] == o["accept"]
+        assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
         assert du < 1e-10
 
 
