@@ -36,6 +36,27 @@ def test_gauge_roundtrip_and_device_rng():
         assert np.abs(c.get_momentum() - P).max() < 1e-15
 
 
+def test_kinetic_energy_and_trajectory_counter():
+    """The kinetic part of get_hamiltonian (constrained last links excluded) and the trajectory
+    counter that selects each trajectory's Philox momenta and uniform."""
+    po = O.make_params(DIMS, mag=2, action=1, beta=2.25, n_stout=0, n_steps=8)
+    U = O.gen_hot(DIMS, 9)
+    with M.Chmc(DIMS, mag=2, seed=21) as c:
+        c.set_gauge(U)
+        P = O.gen_momenta(DIMS, 3, 1)
+        c.init_momentum(P)
+        ko = O.kinetic(po, P)
+        assert abs(c.kinetic_energy() - ko) <= 1e-12 * abs(ko)
+        assert c.traj_counter() == 0
+        c.set_traj_counter(5)
+        assert c.traj_counter() == 5
+        (rec,) = c.trajectory()
+        assert c.traj_counter() == 6
+        k5 = O.kinetic(po, O.gen_momenta(DIMS, 21, 5))
+        assert abs(rec["kinetic_old"] - k5) <= 1e-12 * abs(k5)
+        assert rec["uniform"] == O.gen_uniform(21, 5)
+
+
 @pytest.mark.parametrize("action,mag,n_stout", [
     ("iwasaki", 0, 0), ("wilson", 0, 0), ("iwasaki", 2, 0), ("wilson", 2, 0),
     ("iwasaki", 0, 1), ("iwasaki", 0, 3), ("iwasaki", 2, 3), ("wilson", 2, 1)])
@@ -335,6 +356,23 @@ def test_alias_entry_points():
         code = L.mag_stout_force(c._h, 0, np.zeros((O.volume(DIMS), 4, 3, 3), np.complex128).ctypes.data_as(
             ctypes.POINTER(ctypes.c_double)))
         assert code == _lib.MAG_ERR_STATE
+    # mag_batch_create / mag_batch_run against mag_ensemble_create / mag_run: identical records
+    from mag_b200.field_hmc import make_params
+
+    plist = [make_params((4, 4, 4, 4), n_stout=1, seed=6), make_params((4, 4, 4, 6), n_stout=1, beta=2.4, seed=6)]
+    arr = (_lib.MagParams * 2)(*plist)
+    recs = []
+    for create, run in ((L.mag_batch_create, L.mag_batch_run), (L.mag_ensemble_create, L.mag_run)):
+        h = ctypes.c_void_p()
+        _lib.check(create(arr, 2, ctypes.byref(h)), "create")
+        try:
+            _lib.check(L.mag_gauge_hot_start(h, 3), "hot start")
+            res = (_lib.TrajResult * 4)()
+            _lib.check(run(h, 2, res), "run")
+            recs.append([(r.delta_h, r.accept, r.h_old) for r in res])
+        finally:
+            L.mag_ctx_destroy(h)
+    assert recs[0] == recs[1] and all(np.isfinite(d) for d, _, _ in recs[0])
 
 
 def test_split_ensemble_reproduces_the_single_context():
