@@ -185,6 +185,15 @@ def test_forced_accepts_then_metropolis():
         assert du < 1e-10
 
 
+def test_trajectory_parity_half_length_trajectory():
+    # tau = 0.5 with 4 force-gradient steps (dt = tau / n_steps), one stout level
+    res = _run_pair((4, 4, 4, 6), dict(mag=2, n_steps=4, tau=0.5, n_stout=1), 2)
+    for g, o, du in res:
+        assert abs(g["delta_h"] - o["delta_h"]) < 1e-9
+        assert g["accept"] == o["accept"]
+        assert du < 1e-10
+
+
 def test_trajectory_parity_demon_sequence():
     res = _run_pair((8, 8, 8, 8), dict(mag=2, n_steps=8, accept="demon", e_max=60.0), 3)
     for g, o, _ in res:
@@ -261,6 +270,8 @@ def test_wilson_loops_parity():
             for T in range(1, 5):
                 assert abs(W[R - 1, T - 1] - O.wilson_loop(DIMS, U, (R, 0, 0), T)) < 1e-13
         assert abs(c.avg_wilson_loop((1, 2, 0), 2) - O.wilson_loop(DIMS, U, (1, 2, 0), 2)) < 1e-13
+        for r, T in (((1, 1, 1), 2), ((2, 1, 1), 3)):  # spatial displacements along all three directions
+            assert abs(c.avg_wilson_loop(r, T) - O.wilson_loop(DIMS, U, r, T)) < 1e-13
         c.cold_start()
         assert np.abs(c.wilson_loops(2, 2) - 3.0).max() < 1e-14
 
