@@ -789,6 +789,7 @@ def demon_ensemble_reference_arm(args, params, rank: int, world: int):
 
 def run_demon_ensemble(args, params, rank, world, dist):
     import torch
+    import numpy as np
 
     import mag_b200 as M
     from mag_b200.field_hmc import probe_fma_peak
@@ -807,12 +808,25 @@ def run_demon_ensemble(args, params, rank, world, dist):
             sampler.start()
             time.sleep(0.3)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         res = c.demon_microcanonical_all(args.steps, params["e_max"], seed=seed + 1)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
         dev_s = c.last_measure_ms() / 1e3  # CUDA events on the library's stream around the sweeps
         clocks = sampler.stop() if sampler else None
+        # end to end: every chain's links in from pinned host memory, one sweep keeping them, links out
+        Uh = [torch.empty(V * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(
+            V, 4, 3, 3) for _ in range(n)]
+        for k in range(n):
+            c.get_gauge(k, out=Uh[k])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for j in range(args.steps):
+            for k in range(n):
+                c.set_gauge(Uh[k], chain=k)
+            c.demon_microcanonical_all(1, params["e_max"], seed=seed + 2 + j, update_links=True)
+            for k in range(n):
+                c.get_gauge(k, out=Uh[k])
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
     el = max_over_ranks(dev_s, dist, "cuda")
     wall = max_over_ranks(wall, dist, "cuda")
     if rank != 0:
@@ -839,10 +853,10 @@ def run_demon_ensemble(args, params, rank, world, dist):
                      "flops_per_link": DEMON_FLOPS_PER_LINK,
                      "peak_source": "measured CUDA-core FP64 FMA throughput of the device"},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * n * 4 * V * args.steps / wall, "unit": "link updates/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": n * (48 + 8),
-                "path": "mag_demon_microcanonical_all wall clock (links resident; every chain's demon energies "
-                        "and reunitarisation deviation read back after every sweep)"},
+        "e2e": {"value": world * n * 4 * V * args.steps / wall, "unit": "link updates/s",
+                "h2d_bytes_per_step": n * 576 * V, "d2h_bytes_per_step": n * (576 * V + 48 + 8),
+                "path": "mag_gauge_set per chain + mag_demon_microcanonical_all (one sweep, links kept) + "
+                        "mag_gauge_get per chain, from / to pinned host buffers"},
         "clocks": clocks,
         "gpu_launches": (2 * n + 2) * args.steps,
     }
@@ -851,6 +865,7 @@ def run_demon_ensemble(args, params, rank, world, dist):
 
 def run_demon(args, params, rank, world, dist):
     import torch
+    import numpy as np
 
     import mag_b200 as M
     from mag_b200.field_hmc import probe_fma_peak
@@ -869,12 +884,22 @@ def run_demon(args, params, rank, world, dist):
             sampler.start()
             time.sleep(0.3)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         res = c.demon_microcanonical(args.steps, params["e_max"], seed=seed + 1)
         torch.cuda.synchronize()
-        wall = time.perf_counter() - t0
         dev_s = c.last_measure_ms() / 1e3  # CUDA events on the library's stream around the sweeps
         clocks = sampler.stop() if sampler else None
+        # end to end: links in from pinned host memory, one sweep keeping them, links out
+        Uh = torch.empty(V * 72, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(
+            V, 4, 3, 3)
+        c.get_gauge(out=Uh)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for k in range(args.steps):
+            c.set_gauge(Uh)
+            c.demon_microcanonical(1, params["e_max"], seed=seed + 2 + k, update_links=True)
+            c.get_gauge(out=Uh)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
     el = max_over_ranks(dev_s, dist, "cuda")
     wall = max_over_ranks(wall, dist, "cuda")
     if rank != 0:
@@ -904,10 +929,10 @@ def run_demon(args, params, rank, world, dist):
                      "flops_per_link": DEMON_FLOPS_PER_LINK,
                      "peak_source": "measured CUDA-core FP64 FMA throughput / 148 SMs"},
         "cpu_baseline": cpu,
-        "e2e": {"value": world * args.steps / wall, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 48 + 8,
-                "path": "mag_demon_microcanonical wall clock (links resident; demon energies and the "
-                        "reunitarisation deviation read back after every sweep)"},
+        "e2e": {"value": world * args.steps / wall, "unit": "sweeps/s", "h2d_bytes_per_step": 576 * V,
+                "d2h_bytes_per_step": 576 * V + 48 + 8,
+                "path": "mag_gauge_set + mag_demon_microcanonical (one sweep, links kept) + mag_gauge_get per step "
+                        "from / to a pinned host buffer"},
         "clocks": clocks,
         "gpu_launches": 4 * args.steps,
     }
