@@ -12,6 +12,11 @@ same Philox momenta, so every difference below is the precision's:
   * reversibility: integrate, flip P, integrate again; max |U_back - U_0| and
     |H_back - H_0| for both precisions (the reunitarisation at the end of each
     integration, field-hmc.h:566, is part of the algorithm and included).
+  * with --chain K: K Metropolis trajectories of each precision from the
+    thermalised configuration with the same Philox momenta and uniforms: mean
+    Delta H, mean exp(-Delta H) (1 at equilibrium), acceptance and plaquette of
+    each chain, and how many leading accept decisions the two chains share (while
+    they do, their configurations differ only by the precision's rounding).
 The FP64 path itself matches the CPU oracle to 1e-11 (force) and 1e-9 (Delta H)
 on lattices the oracle can run; this tool extends the comparison to sizes the
 oracle cannot.
@@ -35,6 +40,9 @@ def main(argv=None) -> int:
     ap.add_argument("--therm", type=int, default=6, help="forced-accept FP64 trajectories from the hot start")
     ap.add_argument("--samples", type=int, default=4)
     ap.add_argument("--seed", type=int, default=77)
+    ap.add_argument("--chain", type=int, default=0,
+                    help="also run this many Metropolis trajectories in each precision from the thermalised "
+                         "configuration with the same Philox momenta and uniforms, and compare their statistics")
     a = ap.parse_args(argv)
     dims = tuple(a.dims)
     kw = dict(mag=2, action="iwasaki", beta=a.beta, c1=-0.331, rho=0.1, n_stout=a.n_stout, n_steps=a.steps, tau=1.0,
@@ -83,6 +91,33 @@ def main(argv=None) -> int:
             H2, _ = c.get_hamiltonian()
             out[f"reversibility_{name}"] = {"max_dU": float(np.abs(c.get_gauge() - U0).max()),
                                             "abs_dH": abs(H2 - H0)}
+
+        if a.chain:
+            seq = {}
+            for name, c in (("fp64", c64), ("mixed", c32)):
+                c.set_gauge(U0)
+                c.set_uniforms(None)
+                c.set_traj_counter(5000)
+                recs = [r[0] for r in c.run_chmc(a.chain)]
+                dh = np.array([r["delta_h"] for r in recs])
+                seq[name] = recs
+                out[f"chain_{name}"] = {"trajectories": a.chain, "dH_mean": float(dh.mean()),
+                                        "dH_abs_mean": float(np.abs(dh).mean()),
+                                        "exp_minus_dH_mean": float(np.exp(-dh).mean()),
+                                        "acceptance": float(np.mean([r["accept"] for r in recs])),
+                                        "plaquette_mean": float(np.mean([r["avg_plaquette"] for r in recs]))}
+            same = 0
+            for r64, r32 in zip(seq["fp64"], seq["mixed"]):
+                if r64["accept"] != r32["accept"]:
+                    break
+                same += 1
+            out["chain_identical_accept_prefix"] = same
+            out["chain_dH_diff_max_over_prefix"] = max(
+                [abs(r64["delta_h"] - r32["delta_h"]) for r64, r32 in zip(seq["fp64"][:same], seq["mixed"][:same])],
+                default=0.0)
+            out["chain_plaq_diff_max_over_prefix"] = max(
+                [abs(r64["avg_plaquette"] - r32["avg_plaquette"])
+                 for r64, r32 in zip(seq["fp64"][:same], seq["mixed"][:same])], default=0.0)
     print(json.dumps(out))
     return 0
 
