@@ -168,6 +168,18 @@ int mag_set_stream_index(mag_ctx* ctx, const int64_t* index);
 int mag_traj_counter(mag_ctx* ctx, int64_t* traj);
 int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);
 
+/* ------------------------------------------------ single-matrix operators */
+/* The reference's per-matrix helpers for n matrices at once.  Matrices are host arrays
+   in the memory image of cps::Matrix: 9 complex doubles, row-major, re/im interleaved
+   (double[n][3][3][2]).  Q must be Hermitian and traceless, as the reference assumes;
+   its independent entries (diagonal 0, 1 and the upper triangle) are what is read.
+   Both run on the current device with device buffers allocated for the call.
+   expiQ (field-hmc.h:82-123): out[i] = exp(i Q[i]) by the Cayley-Hamilton closed form. */
+int mag_expiq(const double* q, int64_t n, double* out);
+/* compute_Lambda (field-multi.h:180-269): lambda[i] = the Hermitian traceless part of
+   Gamma(Q[i], SigmaP[i], U[i]), the stout chain rule's Lambda. */
+int mag_compute_lambda(const double* q, const double* sigma, const double* u, int64_t n, double* lambda);
+
 /* --------------------------------------------------- per-link demon sweep */
 /* demon_microcanonical (field-demon.h:25-126) on one chain: n_sweeps sweeps over
    the links in site order (x0 fastest, mu inner) of a copy of the links, each link

@@ -148,6 +148,15 @@ inline double total_rectangular(Lattice& L) {
     check(mag_action(L.ctx(), 0, &p, &r, &s), "mag_action");
     return r;
 }
+// expiQ (field-hmc.h:82-123) of n Hermitian traceless matrices stored as cps::Matrix
+// (18 doubles each, row-major re/im): out[i] = exp(i Q[i])
+inline void expiQ(const double* Q, double* out, long n = 1) { check(mag_expiq(Q, n, out), "mag_expiq"); }
+
+// compute_Lambda (field-multi.h:180-269) of n triples (Q, Sigma', U), cps::Matrix layout
+inline void compute_Lambda(const double* Q, const double* SigmaP, const double* U, double* Lambda, long n = 1) {
+    check(mag_compute_lambda(Q, SigmaP, U, n, Lambda), "mag_compute_lambda");
+}
+
 inline double avg_plaquette(Lattice& L) {
     double v;
     check(mag_plaquette(L.ctx(), 0, &v), "mag_plaquette");

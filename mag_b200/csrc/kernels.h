@@ -158,6 +158,12 @@ void launch_payload_to_links(const double* payload, int two_row, int off, int V,
                              cudaStream_t s);
 void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, double* payload, cudaStream_t s);
 
+// ---- single-matrix operators, batched (kernels_matrix.cu): n matrices of 9 complex doubles each,
+// row-major, on the device; Q Hermitian traceless (its independent entries are read)
+void launch_expiq(const double* q, long n, double* out, cudaStream_t s);
+void launch_compute_lambda(const double* q, const double* sigma, const double* u, long n, double* lam,
+                           cudaStream_t s);
+
 // ---- per-link demon sweep (kernels_demon.cu)
 constexpr int kDemonPaths = 168;   // staple paths per link: 6 plaquette, 18 rectangle, 72 chair, 72 twist
 constexpr int kDemonWindow = 384;  // capacity of the per-site link window (353 used)

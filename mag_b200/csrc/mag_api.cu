@@ -596,6 +596,38 @@ struct mag_ctx {
 };
 
 // ======================================================================= C ABI
+namespace {
+
+// a device buffer released on every return path
+struct DeviceBuffer {
+    void* p = nullptr;
+    ~DeviceBuffer() {
+        if (p) cudaFree(p);
+    }
+};
+
+// n 3x3 complex matrices (144 bytes each) in from the host, `run` on the device, n out
+template <typename Run>
+int matrix_op(const char* name, const double* const* in, int nin, int64_t n, double* out, Run run) {
+    for (int k = 0; k < nin; k++)
+        if (!in[k]) return fail(MAG_ERR_ARG, std::string(name) + ": null input");
+    if (!out || n < 0) return fail(MAG_ERR_ARG, std::string(name) + ": bad argument");
+    if (n == 0) return MAG_OK;
+    const size_t bytes = (size_t)n * 144;
+    DeviceBuffer din[3], dout;
+    for (int k = 0; k < nin; k++) {
+        MAG_CUDA(cudaMalloc(&din[k].p, bytes));
+        MAG_CUDA(cudaMemcpy(din[k].p, in[k], bytes, cudaMemcpyHostToDevice));
+    }
+    MAG_CUDA(cudaMalloc(&dout.p, bytes));
+    run((const double*)din[0].p, (const double*)din[1].p, (const double*)din[2].p, (double*)dout.p);
+    MAG_CUDA(cudaGetLastError());
+    MAG_CUDA(cudaMemcpy(out, dout.p, bytes, cudaMemcpyDeviceToHost));
+    return MAG_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* mag_last_error(void) { return g_last_error.c_str(); }
@@ -1244,6 +1276,21 @@ int mag_graph_kernel_count(mag_ctx* ctx, int* kernels) {
     MAG_TRY(ctx->build_graph());
     *kernels = ctx->graph_kernels;
     return MAG_OK;
+}
+
+int mag_expiq(const double* q, int64_t n, double* out) {
+    const double* in[1] = {q};
+    return matrix_op("mag_expiq", in, 1, n, out, [&](const double* dq, const double*, const double*, double* o) {
+        launch_expiq(dq, (long)n, o, 0);
+    });
+}
+
+int mag_compute_lambda(const double* q, const double* sigma, const double* u, int64_t n, double* lambda) {
+    const double* in[3] = {q, sigma, u};
+    return matrix_op("mag_compute_lambda", in, 3, n, lambda,
+                     [&](const double* dq, const double* ds, const double* du, double* o) {
+                         launch_compute_lambda(dq, ds, du, (long)n, o, 0);
+                     });
 }
 
 int mag_probe_fma_peak(int precision, double* tflops) {

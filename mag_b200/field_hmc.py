@@ -353,6 +353,29 @@ class Chmc:
         return v.value
 
 
+def _matrices(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.complex128)
+    assert a.shape[-2:] == (3, 3)
+    return a
+
+
+def expiq(Q) -> np.ndarray:
+    """expiQ (field-hmc.h:82-123) of Hermitian traceless matrices Q[..., 3, 3] on the GPU."""
+    q = _matrices(Q)
+    out = np.empty_like(q)
+    check(_lib.load().mag_expiq(_dp(q), q.size // 9, _dp(out)), "mag_expiq")
+    return out
+
+
+def compute_lambda(Q, SigmaP, U) -> np.ndarray:
+    """compute_Lambda (field-multi.h:180-269) of triples (Q, Sigma', U)[..., 3, 3] on the GPU."""
+    q, s, u = _matrices(Q), _matrices(SigmaP), _matrices(U)
+    assert q.shape == s.shape == u.shape
+    out = np.empty_like(q)
+    check(_lib.load().mag_compute_lambda(_dp(q), _dp(s), _dp(u), q.size // 9, _dp(out)), "mag_compute_lambda")
+    return out
+
+
 def probe_fma_peak(precision: str = "fp64") -> float:
     """Measured CUDA-core FMA throughput of the current device (TFLOP/s, 2 flops per FMA)."""
     v = ctypes.c_double()

@@ -36,6 +36,37 @@ def test_gauge_roundtrip_and_device_rng():
         assert np.abs(c.get_momentum() - P).max() < 1e-15
 
 
+def _herm_traceless(rng, scale):
+    A = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+    H = (A + A.conj().T) / 2
+    return (H - np.trace(H).real / 3 * np.eye(3)) * scale
+
+
+def test_expiq_and_compute_lambda_match_the_oracle():
+    """mag_expiq / mag_compute_lambda (the reference's expiQ and compute_Lambda for n matrices)
+    against the oracle's literal restatement: Q of scale 0.01 to 2.5 (both signs of det Q, so the
+    reflection branch too) and Q = 0 (the c1 = 0 branch)."""
+    from mag_b200.field_hmc import compute_lambda, expiq
+
+    rng = np.random.default_rng(5)
+    n = 200
+    Q = np.array([_herm_traceless(rng, (0.01, 0.1, 1.0, 2.5)[i % 4]) for i in range(n)])
+    Q[0] = 0.0
+    S = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
+    U = O.gen_hot((2, 2, 4, 4), 3).reshape(-1, 3, 3)[:n]
+    E = expiq(Q)
+    Eo = np.array([O.expiQ(q) for q in Q])
+    assert np.array_equal(E[0], np.eye(3))
+    dE = np.abs(E - Eo).max()
+    L = compute_lambda(Q, S, U)
+    Lo = np.array([O.compute_lambda(q, s, u) for q, s, u in zip(Q, S, U)])
+    assert np.all(L[0] == 0)
+    dL = max(np.abs(L[i] - Lo[i]).max() / max(1.0, np.abs(Lo[i]).max()) for i in range(n))
+    assert dE < 1e-14
+    assert dL < 1e-12
+    assert sum(1 for q in Q if np.linalg.det(q).real < 0) > 10  # the reflection branch is exercised
+
+
 def test_kinetic_energy_and_trajectory_counter():
     """The kinetic part of get_hamiltonian (constrained last links excluded) and the trajectory
     counter that selects each trajectory's Philox momenta and uniform."""
