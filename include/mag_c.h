@@ -176,6 +176,9 @@ int mag_set_traj_counter(mag_ctx* ctx, int64_t traj);
    Both run on the current device with device buffers allocated for the call.
    expiQ (field-hmc.h:82-123): out[i] = exp(i Q[i]) by the Cayley-Hamilton closed form. */
 int mag_expiq(const double* q, int64_t n, double* out);
+/* DexpiQ (field-multi.h:90-178): out[i] = the derivative of exp(i Q) at Q[i] in the
+   direction DQ[i] (any 3x3 matrix); zero where Q[i] = 0, as the reference returns. */
+int mag_dexpiq(const double* q, const double* dq, int64_t n, double* out);
 /* compute_Lambda (field-multi.h:180-269): lambda[i] = the Hermitian traceless part of
    Gamma(Q[i], SigmaP[i], U[i]), the stout chain rule's Lambda. */
 int mag_compute_lambda(const double* q, const double* sigma, const double* u, int64_t n, double* lambda);

@@ -152,6 +152,11 @@ inline double total_rectangular(Lattice& L) {
 // (18 doubles each, row-major re/im): out[i] = exp(i Q[i])
 inline void expiQ(const double* Q, double* out, long n = 1) { check(mag_expiq(Q, n, out), "mag_expiq"); }
 
+// DexpiQ (field-multi.h:90-178) of n pairs (Q, DQ), cps::Matrix layout
+inline void DexpiQ(const double* Q, const double* DQ, double* out, long n = 1) {
+    check(mag_dexpiq(Q, DQ, n, out), "mag_dexpiq");
+}
+
 // compute_Lambda (field-multi.h:180-269) of n triples (Q, Sigma', U), cps::Matrix layout
 inline void compute_Lambda(const double* Q, const double* SigmaP, const double* U, double* Lambda, long n = 1) {
     check(mag_compute_lambda(Q, SigmaP, U, n, Lambda), "mag_compute_lambda");

@@ -134,6 +134,7 @@ SIGNATURES = {
                                  _DP, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _DP],
     "mag_expiq": [_DP, ctypes.c_int64, _DP],
     "mag_compute_lambda": [_DP, _DP, _DP, ctypes.c_int64, _DP],
+    "mag_dexpiq": [_DP, _DP, ctypes.c_int64, _DP],
     "mag_demon_microcanonical_all": [_CTX, ctypes.c_int, ctypes.c_double, ctypes.c_uint64, ctypes.c_int, _DP,
                                      ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _DP],
     "mag_reunitarize": [_CTX, _DP],

@@ -161,6 +161,7 @@ void launch_links_to_payload(LinkPlanes<double> U, int two_row, int off, int V, 
 // ---- single-matrix operators, batched (kernels_matrix.cu): n matrices of 9 complex doubles each,
 // row-major, on the device; Q Hermitian traceless (its independent entries are read)
 void launch_expiq(const double* q, long n, double* out, cudaStream_t s);
+void launch_dexpiq(const double* q, const double* dq, long n, double* out, cudaStream_t s);
 void launch_compute_lambda(const double* q, const double* sigma, const double* u, long n, double* lam,
                            cudaStream_t s);
 

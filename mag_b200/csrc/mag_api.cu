@@ -1285,6 +1285,13 @@ int mag_expiq(const double* q, int64_t n, double* out) {
     });
 }
 
+int mag_dexpiq(const double* q, const double* dq, int64_t n, double* out) {
+    const double* in[2] = {q, dq};
+    return matrix_op("mag_dexpiq", in, 2, n, out, [&](const double* d0, const double* d1, const double*, double* o) {
+        launch_dexpiq(d0, d1, (long)n, o, 0);
+    });
+}
+
 int mag_compute_lambda(const double* q, const double* sigma, const double* u, int64_t n, double* lambda) {
     const double* in[3] = {q, sigma, u};
     return matrix_op("mag_compute_lambda", in, 3, n, lambda,

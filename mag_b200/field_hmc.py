@@ -367,6 +367,15 @@ def expiq(Q) -> np.ndarray:
     return out
 
 
+def dexpiq(Q, DQ) -> np.ndarray:
+    """DexpiQ (field-multi.h:90-178): derivative of exp(iQ) at Q[..., 3, 3] along DQ, on the GPU."""
+    q, d = _matrices(Q), _matrices(DQ)
+    assert q.shape == d.shape
+    out = np.empty_like(q)
+    check(_lib.load().mag_dexpiq(_dp(q), _dp(d), q.size // 9, _dp(out)), "mag_dexpiq")
+    return out
+
+
 def compute_lambda(Q, SigmaP, U) -> np.ndarray:
     """compute_Lambda (field-multi.h:180-269) of triples (Q, Sigma', U)[..., 3, 3] on the GPU."""
     q, s, u = _matrices(Q), _matrices(SigmaP), _matrices(U)

@@ -43,10 +43,11 @@ def _herm_traceless(rng, scale):
 
 
 def test_expiq_and_compute_lambda_match_the_oracle():
-    """mag_expiq / mag_compute_lambda (the reference's expiQ and compute_Lambda for n matrices)
+    """mag_expiq / mag_dexpiq / mag_compute_lambda (the reference's expiQ, DexpiQ and compute_Lambda
+    for n matrices)
     against the oracle's literal restatement: Q of scale 0.01 to 2.5 (both signs of det Q, so the
     reflection branch too) and Q = 0 (the c1 = 0 branch)."""
-    from mag_b200.field_hmc import compute_lambda, expiq
+    from mag_b200.field_hmc import compute_lambda, dexpiq, expiq
 
     rng = np.random.default_rng(5)
     n = 200
@@ -64,6 +65,12 @@ def test_expiq_and_compute_lambda_match_the_oracle():
     dL = max(np.abs(L[i] - Lo[i]).max() / max(1.0, np.abs(Lo[i]).max()) for i in range(n))
     assert dE < 1e-14
     assert dL < 1e-12
+    D = rng.standard_normal((n, 3, 3)) + 1j * rng.standard_normal((n, 3, 3))
+    G = dexpiq(Q, D)
+    Go = np.array([O.dexpiQ(q, d) for q, d in zip(Q, D)])
+    assert np.all(G[0] == 0)
+    dG = max(np.abs(G[i] - Go[i]).max() / max(1.0, np.abs(Go[i]).max()) for i in range(n))
+    assert dG < 1e-12
     assert sum(1 for q in Q if np.linalg.det(q).real < 0) > 10  # the reflection branch is exercised
 
 
