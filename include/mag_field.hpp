@@ -113,18 +113,30 @@ class Lattice {
 
 // ------------------------------------------------------------ field-hmc.h
 // init_momentum (field-hmc.h:675-693): host momenta, or the Philox stream of trajectory `traj`
+// with the reference's width sqrt(m) (m = 1 on the HMC path; other m scale on the host)
 inline void init_momentum(Lattice& L, const std::vector<double>& P) {
     check(mag_momentum_set(L.ctx(), 0, P.data()), "mag_momentum_set");
 }
-inline void init_momentum(Lattice& L, uint64_t traj) { check(mag_momentum_refresh(L.ctx(), traj), "mag_momentum_refresh"); }
+inline void init_momentum(Lattice& L, uint64_t traj, double m = 1.) {
+    check(mag_momentum_refresh(L.ctx(), traj), "mag_momentum_refresh");
+    if (m != 1.) {
+        std::vector<double> P((size_t)L.volume() * 72);
+        check(mag_momentum_get(L.ctx(), 0, P.data()), "mag_momentum_get");
+        const double sig = std::sqrt(m);
+        for (double& v : P) v *= sig;
+        check(mag_momentum_set(L.ctx(), 0, P.data()), "mag_momentum_set");
+    }
+}
 
 // get_force (field-hmc.h:339-425) into a host AoS buffer
 inline void get_force(std::vector<double>& F, Lattice& L) {
     F.resize((size_t)L.volume() * 72);
     check(mag_gauge_force(L.ctx(), 0, F.data()), "mag_gauge_force");
 }
-// evolve_momentum (field-hmc.h:427-440) with the force of the current links
-inline void evolve_momentum(Lattice& L, double dt) { check(mag_evolve_momentum(L.ctx(), dt), "mag_evolve_momentum"); }
+// evolve_momentum (field-hmc.h:427-440) with the force of the current links: P += F dt m
+inline void evolve_momentum(Lattice& L, double dt, double m = 1.) {
+    check(mag_evolve_momentum(L.ctx(), dt * m), "mag_evolve_momentum");
+}
 // evolve_gauge_field (field-hmc.h:442-482)
 inline void evolve_gauge_field(Lattice& L, double dt) { check(mag_evolve_gauge(L.ctx(), dt), "mag_evolve_gauge"); }
 // force_gradient_integrator (field-hmc.h:525-567)
