@@ -5,10 +5,12 @@ A step is one HMC trajectory of the workload (momentum refresh, H_old, the
 force-gradient molecular dynamics, reunitarisation, H_new, accept/reject),
 replayed as one CUDA graph; for the ensemble workload a step advances every
 chain by one trajectory and `value` counts chain-trajectories.  The default
-workload is the 16^3 x 32 lattice, Iwasaki beta = 2.25 (c1 = -0.331), three
-stout levels rho = 0.1, twelve force-gradient steps of tau = 1, constraint
-magnification 2, Metropolis accept, plain FP64; the same lattice in mixed
-precision is measured beside it.
+workload is the 32^4 lattice, Iwasaki beta = 2.25 (c1 = -0.331), three stout
+levels rho = 0.1, sixteen force-gradient steps of tau = 1, constraint
+magnification 2, Metropolis accept: `value` is the plain FP64 path and the
+same lattice in mixed precision is measured beside it (`mixed`, with its
+speed-up over FP64).  On one GPU the default run also measures the 16^3 x 32
+FP64 configuration (12 FG steps) and the 96-chain ensemble as sub-keys.
 
   python bench.py [--gpus N --steps K --warmup W] [--workload NAME] [--impl reference]
 
@@ -19,12 +21,16 @@ the data path (the only collective is the max over ranks of the timing).
 --impl reference times the reference's algorithm on the host cores: the
 reference itself cannot be built here (it needs CPS, Qlattice, QMP, MPI), so
 this is the FP64 CPU restatement in oracle/ (OpenMP over sites, as the
-reference's field-hmc.h:385), run on a bounded sample and extrapolated.
+reference's field-hmc.h:385).  Each of its steps is one full-lattice force
+evaluation (the unit a trajectory repeats 4n times); `ms_per_step` is that
+timed unit and `value` the trajectory rate extrapolated from it, labelled as
+such in `value_basis`.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -74,7 +80,7 @@ WORKLOADS = {
     "demon_ensemble_148x8x8x8x8": dict(dims=(8, 8, 8, 8), nchains=148, beta=2.25, n_stout=0, n_steps=1,
                                        precision="fp64", kind="demon_ensemble", e_max=50.0),
 }
-DEFAULT = "16x16x16x32_iwasaki_3stout"
+DEFAULT = "32x32x32x32_iwasaki_3stout"
 COMMON = dict(mag=2, action="iwasaki", c1=-0.331, rho=0.1, tau=1.0, accept="metropolis", integrator="fg")
 
 # algorithmic flops per site of one launch, reference (gather) formulation:
@@ -119,6 +125,7 @@ def parse():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-sub", action="store_true", help="skip the other configurations of the default run")
     return ap.parse_args()
 
 
@@ -258,7 +265,79 @@ def cpu_sample(params: dict) -> dict:
             "cores": O.lib().mo_get_threads()}
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (the CPU baseline runs on it)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def extrapolation_check() -> dict | None:
+    """Whole oracle trajectories against the extrapolation from their parts, measured on one host
+    when tests/golden/run_16x16x16x32_3stout.json was written (16^3 x 32, 3 stout levels, 12 FG
+    steps): the factor that the trajectory rate of the CPU legs rests on."""
+    path = os.path.join(ROOT, "tests", "golden", "run_16x16x16x32_3stout.json")
+    if not os.path.exists(path):
+        return None
+    t = json.load(open(path))["timing"]
+    meas = statistics.median(t["measured_trajectory_s"])
+    return {"lattice": "16x16x16x32", "threads": t["threads"], "cpu": t["cpu"],
+            "measured_trajectory_s_median": meas, "extrapolated_trajectory_s": t["extrapolated_trajectory_s"],
+            "measured_over_extrapolated": meas / t["extrapolated_trajectory_s"],
+            "trajectories": len(t["measured_trajectory_s"])}
+
+
+def reference_whole_trajectories(args, params, world, dims, U):
+    """Lattices whose whole run fits in two minutes of host time: each step is one whole oracle
+    trajectory (momentum draw, H_old, the integrator, reunitarisation, H_new, accept), measured."""
+    import oracle as O
+
+    po = O.make_params(dims, mag=params["mag"], action=1, beta=params["beta"], c1=params["c1"], rho=params["rho"],
+                       n_stout=params["n_stout"], tau=params["tau"], n_steps=params["n_steps"],
+                       accept=1 if params.get("accept") == "demon" else 0, e_max=params.get("e_max", 100.0),
+                       n_forced=args.warmup)
+    demon = [0.0, 0.0]
+    ts = []
+    for t in range(args.warmup + args.steps):
+        P = O.gen_momenta(dims, 1, t)
+        u = O.gen_uniform(1, t)
+        t0 = time.perf_counter()
+        U, r = O.trajectory(po, t, U, P, u, demon)
+        dt = time.perf_counter() - t0
+        demon = r["demon"]
+        if t >= args.warmup:
+            ts.append(dt)
+    t_traj = statistics.fmean(ts)
+    value = 1.0 / t_traj
+    lat = "x".join(map(str, dims))
+    cores = O.lib().mo_get_threads()
+    line = {
+        "metric": METRIC, "value": value, "unit": "traj/s", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_traj * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
+        "config": config_of(args.workload, params, world),
+        "step_definition": f"one whole oracle trajectory of the {lat} lattice (measured, not extrapolated)",
+        "value_basis": {"kind": "measured whole trajectories", "t_traj_s_each": ts},
+        "cpu_baseline": {"value": value, "unit": "traj/s", "cores": cores, "kind": "port", "cpu": cpu_model(),
+                         "sample": f"{args.steps} whole trajectories of the {lat} lattice (FP64 oracle port, "
+                                   f"{cores} OpenMP threads), after {args.warmup} untimed ones"},
+        "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def reference_arm(args, params, rank: int, world: int):
+    """The oracle (FP64, OpenMP over sites on every host thread) on the workload's lattice.  A step
+    is one full-lattice force evaluation, the unit a trajectory repeats 4n times; the link update
+    and the Hamiltonian (4n + 1 and 2 per trajectory, about 2% of it) are timed once beforehand.
+    `ms_per_step` is the timed unit; `value` is the trajectory rate extrapolated from it."""
     if rank != 0:
         return
     import oracle as O
@@ -272,6 +351,13 @@ def reference_arm(args, params, rank: int, world: int):
     t0 = time.perf_counter()
     O.hamiltonian(po, U, P)
     t_ham = time.perf_counter() - t0
+    n = params["n_steps"]
+    nchain = len(params["chains"]) if "chains" in params else 1
+    t0 = time.perf_counter()
+    O.force(po, U)
+    t_est = 4 * n * (time.perf_counter() - t0) + (4 * n + 1) * t_evolve + 2 * t_ham
+    if nchain == 1 and t_est * (args.steps + args.warmup) < 120.0:
+        return reference_whole_trajectories(args, params, world, dims, U)
     for _ in range(args.warmup):
         O.force(po, U)
     ts = []
@@ -279,22 +365,29 @@ def reference_arm(args, params, rank: int, world: int):
         t0 = time.perf_counter()
         O.force(po, U)
         ts.append(time.perf_counter() - t0)
-    t_force = statistics.median(ts)
-    n = params["n_steps"]
+    t_force = statistics.fmean(ts)
     traj_s = 4 * n * t_force + (4 * n + 1) * t_evolve + 2 * t_ham
-    nchain = len(params["chains"]) if "chains" in params else 1
     # ensemble: every chain's trajectory costs (its volume / the sampled volume) of the sampled one
     traj_s_job = traj_s * total_sites(params) / site_count(dims)
     value = nchain / traj_s_job
-    sample = (f"each step = one {params['n_stout']}-level stout Iwasaki force evaluation of a "
-              f"{'x'.join(map(str, dims))} lattice (FP64 oracle port); trajectory = {4 * n} force evals + "
-              f"{4 * n + 1} link updates + 2 Hamiltonians" + (", scaled by volume to all chains" if nchain > 1 else ""))
+    lat = "x".join(map(str, dims))
+    cores = O.lib().mo_get_threads()
+    sample = (f"each step = one {params['n_stout']}-level stout Iwasaki force evaluation of the {lat} lattice "
+              f"(FP64 oracle port, {cores} OpenMP threads); trajectory rate extrapolated from it: {4 * n} force "
+              f"evaluations + {4 * n + 1} link updates + 2 Hamiltonians"
+              + (", scaled by volume to all chains" if nchain > 1 else ""))
     line = {
         "metric": METRIC, "value": value, "unit": "traj/s", "impl": "reference", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": traj_s_job * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_force * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic: Philox Haar hot start",
         "config": config_of(args.workload, params, world),
-        "cpu_baseline": {"value": value, "unit": "traj/s", "cores": O.lib().mo_get_threads(), "kind": "port",
+        "step_definition": f"one full-lattice force evaluation of the {lat} lattice (the timed unit)",
+        "value_basis": {"kind": "extrapolated from the timed force evaluations", "force_evals_per_traj": 4 * n,
+                        "link_updates_per_traj": 4 * n + 1, "hamiltonians_per_traj": 2,
+                        "t_force_s": t_force, "t_force_s_each": ts, "t_link_update_s": t_evolve,
+                        "t_hamiltonian_s": t_ham, "trajectory_s": traj_s_job,
+                        "check_whole_trajectories": extrapolation_check()},
+        "cpu_baseline": {"value": value, "unit": "traj/s", "cores": cores, "kind": "port", "cpu": cpu_model(),
                          "sample": sample},
         "e2e": {"value": value, "unit": "traj/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "force_evals_per_s": 1.0 / t_force,
@@ -328,6 +421,38 @@ def make_ctx(M, params, seed, precision, n_forced):
     if "chains" in params:
         return M.Chmc(chains=params["chains"], seed=seed, **kw)
     return M.Chmc(params["dims"], seed=seed, **kw)
+
+
+def sub_run(M, workload: str, precisions, args) -> dict:
+    """One GPU, no collective: W forced-accept trajectories, then K timed ones (CUDA events around
+    the graph launches) per precision; chain-trajectories/s for an ensemble."""
+    import torch
+
+    params = workload_params(workload)
+    nchain = len(params["chains"]) if "chains" in params else 1
+    out = {"workload": workload, "fg_steps": params["n_steps"], "stout_levels": params["n_stout"]}
+    if "chains" in params:
+        out["chains"] = nchain
+        out["sites"] = total_sites(params)
+    else:
+        out["lattice"] = "x".join(map(str, params["dims"]))
+    for prec in precisions:
+        c = make_ctx(M, params, rank_seed(0), prec, args.warmup)
+        c.hot_start(rank_seed(0))
+        if args.warmup:
+            c.run_chmc(args.warmup)
+        torch.cuda.synchronize()
+        recs = c.run_chmc(args.steps)
+        ms = c.last_run_ms()
+        out[prec] = {"value": nchain * args.steps / (ms / 1e3),
+                     "unit": "chain-traj/s" if nchain > 1 else "traj/s", "ms_per_step": ms / args.steps,
+                     "acceptance": statistics.fmean(r[k]["accept"] for r in recs for k in range(nchain)),
+                     "delta_h_mean": statistics.fmean(r[k]["delta_h"] for r in recs for k in range(nchain)),
+                     "graph_kernels_per_step": c.graph_kernel_count()}
+        c.close()
+    if "fp64" in out and "mixed" in out:
+        out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    return out
 
 
 def run_gpu(args, params, rank, world, dist):
@@ -410,21 +535,23 @@ def run_gpu(args, params, rank, world, dist):
     t_force_eval = c64.time_force(3)
     prec_key = "fp64" if head_prec == "fp64" else "fp32"
     peak = probe_fma_peak(prec_key)
-    achieved = FLOPS_PER_SITE[dom] * V / (kt[dom] * 1e-3) / 1e12
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get(f"{args.workload}:{head_prec}:{dom}")
+    # achieved = flops the kernel executes per launch (two-row SU(3) and Hermitian products, confirmed
+    # by ncu's FMA/ADD/MUL instruction counts) / its CUDA-event launch time
     executed = EXECUTED_FLOPS_PER_SITE[dom] * V / (kt[dom] * 1e-3) / 1e12
-    roofline = {"bound": prec_key, "kernel": dom, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic,
-                "executed": {"achieved": executed, "frac": executed / peak,
-                             "flops_per_site": EXECUTED_FLOPS_PER_SITE[dom],
-                             "note": "flops the kernel executes after reassociation (two-row SU(3) and "
-                                     "Hermitian products); `achieved` counts the reference's gather formulation"},
+    gather = FLOPS_PER_SITE[dom] * V / (kt[dom] * 1e-3) / 1e12
+    roofline = {"bound": prec_key, "kernel": dom, "achieved": executed, "peak": peak, "unit": "TFLOP/s",
+                "frac": executed / peak, "traffic": traffic, "flops_per_site": EXECUTED_FLOPS_PER_SITE[dom],
+                "algorithmic_equiv": {"achieved": gather, "frac": gather / peak, "flops_per_site": FLOPS_PER_SITE[dom],
+                                      "note": "the reference's gather formulation (85 / 67 products per link); "
+                                              "the kernels execute fewer flops, so this can exceed 1"},
                 "peak_source": f"measured CUDA-core {prec_key.upper()} FMA throughput (mag_probe_fma_peak)",
-                "flops_per_site": FLOPS_PER_SITE[dom], "launch_ms": kt[dom],
-                "kernel_ms": kt, "force_eval_ms": t_force_eval, "tuned_min_blocks": c64.autotune(3)}
+                "launch_ms": kt[dom], "kernel_ms": kt,
+                "executed_frac": {k: EXECUTED_FLOPS_PER_SITE[k] * V / (kt[k] * 1e-3) / 1e12 / peak for k in names},
+                "force_eval_ms": t_force_eval, "tuned": c64.autotune(3)}
     ev_ms = c64.time_kernel("evolve", 5)
     bytes_evolve = V * 4 * (144 + 144 + 64) + (V * 4 * 72 if head_prec == "mixed" else 0)
     peaks = {}
@@ -497,6 +624,7 @@ def run_gpu(args, params, rank, world, dist):
         vm = job_chains * args.steps / (msm / 1e3)
         mixed = {"value": vm, "unit": "traj/s", "ms_per_step": msm / args.steps, "speedup_vs_fp64": vm / value,
                  "delta_h_mean": statistics.fmean(r[0]["delta_h"] for r in recm),
+                 "exp_minus_delta_h_mean": statistics.fmean(math.exp(-r[0]["delta_h"]) for r in recm),
                  "acceptance": statistics.fmean(r[0]["accept"] for r in recm),
                  "plaquette": recm[-1][0]["avg_plaquette"],
                  "force_eval_ms": cm.time_force(3)}
@@ -507,12 +635,19 @@ def run_gpu(args, params, rank, world, dist):
         s = cpu_sample(params)
         vol_ratio = V / site_count(oracle_params(params)[0])
         cpu = {"value": nchain / (s["traj_s"] * vol_ratio), "unit": "traj/s", "cores": s["cores"], "kind": "port",
+               "cpu": cpu_model(), "extrapolation_check": extrapolation_check(),
                "sample": (f"oracle FP64 port, OpenMP: one force evaluation ({s['t_force']:.2f} s), one link update "
                           f"({s['t_evolve']:.2f} s) and one Hamiltonian ({s['t_ham']:.2f} s) of the "
                           f"{'x'.join(map(str, oracle_params(params)[0]))} lattice, extrapolated to {4 * n} force "
                           f"evals + {4 * n + 1} updates + 2 Hamiltonians per trajectory"
                           + (" and by volume to all chains" if nchain > 1 else "")),
                "force_evals_per_s": 1.0 / s["t_force"]}
+
+    # the other HMC configurations, measured beside the headline on one GPU
+    sub = {}
+    if world == 1 and args.workload == DEFAULT and not args.no_sub:
+        sub["config2_16x16x16x32"] = sub_run(M, "16x16x16x32_iwasaki_3stout", ("fp64", "mixed"), args)
+        sub["ensemble_96chains"] = sub_run(M, "ensemble_96chains", ("mixed",), args)
 
     if rank != 0:
         return
@@ -526,10 +661,13 @@ def run_gpu(args, params, rank, world, dist):
         "force_evals_per_s": job_chains * 4 * n * args.steps / (ms64 / 1e3),
         "site_updates_per_s": job_sites * 4 * n * args.steps / (ms64 / 1e3),
         "delta_h_mean": statistics.fmean(dh), "delta_h_abs_mean": statistics.fmean(abs(x) for x in dh),
+        "exp_minus_delta_h_mean": statistics.fmean(math.exp(-x) for x in dh),
         "acceptance": statistics.fmean(acc), "plaquette": plaq,
         "mixed": mixed, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": kernels_per_traj * args.steps,
     }
+    if sub:
+        line["other_configs"] = sub
     if wl:
         line["wilson_loops_ms_per_step"] = wl_ms / args.steps
     print(json.dumps(line), flush=True)

@@ -266,9 +266,11 @@ int mag_nersc_read_header(const char* path, mag_nersc_info* info);
    in one static device array of MAG_NOALLOC_MAX_SITES / 256 * 2 double-double
    entries (2 MiB), held by every GPU that loads the library until exit, and
    lattices larger than MAG_NOALLOC_MAX_SITES sites are rejected with
-   MAG_ERR_ARG.  The first call on a device looks up that array's address;
-   make that first call before any stream capture.  Calls share the array, so
-   calls that overlap on the GPU race with each other. */
+   MAG_ERR_ARG.  The first call on a device looks up that array's address
+   (again when it is called under another context of that device); make that
+   first call before any stream capture.  Calls share the array, so calls that
+   overlap on the GPU race with each other.  Like every mag_ctx, it does not
+   survive cudaDeviceReset of its device within one process. */
 #define MAG_NOALLOC_MAX_SITES (1 << 24)
 int mag_action_sums_noalloc(const int dims[4], const double* d_links, double* d_sums, void* stream);
 

@@ -12,6 +12,7 @@
 // holds that array until the process exits, and every call on a device shares
 // it: two calls that overlap on the GPU (different streams, no ordering
 // between them) race on it and both results are then undefined.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -38,6 +39,7 @@ __device__ __align__(256) dd2 g_noalloc_partials[2 * kMaxBlocks];
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 dd2* g_partials_ptr[kMaxDevices] = {};
+CUcontext g_partials_ctx[kMaxDevices] = {};  // the context each cached address belongs to
 
 __device__ __forceinline__ dd2 na_two_sum(double a, double b) {
     const double s = a + b, bp = s - a;
@@ -133,20 +135,41 @@ int na_fail(int code, const std::string& msg) {
     return code;
 }
 
+// The calling thread's current CUDA context, through the driver entry point
+// the runtime hands out (no link-time dependence on the driver library).
+typedef CUresult (*ctx_get_current_fn)(CUcontext*);
+CUcontext current_context() {
+    static ctx_get_current_fn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        fn = reinterpret_cast<ctx_get_current_fn>(p);
+    }
+    CUcontext c = nullptr;
+    return fn(&c) == CUDA_SUCCESS ? c : nullptr;
+}
+
 // Device address of the static partials for the current device.  The first
-// call on a device looks it up (cudaGetSymbolAddress); later calls reuse it.
+// call on a device (in a given context) looks it up with cudaGetSymbolAddress;
+// later calls in the same context reuse it.  A call made under another
+// context on the same device looks the address up again for that context.
 int partials_for_current_device(dd2** out) {
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return na_fail(MAG_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return na_fail(MAG_ERR_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_partials_ptr[dev]) {
+    if (!g_partials_ptr[dev] || g_partials_ctx[dev] != current_context()) {
         void* p = nullptr;
+        // also makes the device's primary context current if no context was
         e = cudaGetSymbolAddress(&p, g_noalloc_partials);
         if (e != cudaSuccess || !p)
             return na_fail(MAG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
         g_partials_ptr[dev] = static_cast<dd2*>(p);
+        g_partials_ctx[dev] = current_context();
     }
     *out = g_partials_ptr[dev];
     return MAG_OK;

@@ -40,3 +40,7 @@ def test_cpp_driver_matches_python_api(tmp_path):
     assert abs(res["cplaq_after"] - res["cplaq_before"]) < 1e-12
     # export_config_nersc -> import_config_nersc (two-row file, third row rebuilt) resumes the same field
     assert abs(res["plaq_reload"] - res["plaq"]) < 1e-13
+    # init_momentum(L, traj, m = 4) draws exactly twice the m = 1 momenta (width sqrt(m));
+    # evolve_momentum(L, dt = 0.1, m = 2.5) adds F dt m = 0.25 F to every component
+    assert res["sqrt_m_exact"] == 1
+    assert res["fmax"] > 0.1 and res["kick_err"] < 1e-14 * max(1.0, res["fmax"])
