@@ -31,12 +31,27 @@ def main(argv=None) -> int:
     ap.add_argument("--nvtx", action="store_true",
                     help="wrap each --kernels timing loop in an NVTX range time_<kernel> (for ncu --nvtx-include)")
     ap.add_argument("--n-steps", type=int, default=12, help="force-gradient steps per trajectory")
+    ap.add_argument("--wilson", type=int, default=0, metavar="RT",
+                    help="also time Wilson loops R, T <= RT (inside an NVTX range 'wilson' with --nvtx)")
+    ap.add_argument("--ensemble", action="store_true",
+                    help="the 96-chain ensemble (48 x 8^4, 32 x 12^4, 16 x 16^4, beta ~ U[2.0, 2.6) from seed 4) "
+                         "in place of --dims")
     ap.add_argument("--traj", type=int, default=0,
                     help="also run this many trajectories after one warm-up trajectory (inside an NVTX range "
                          "'trajectories' with --nvtx) and report their device time")
     a = ap.parse_args(argv)
-    with M.Chmc(tuple(a.dims), mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1, n_steps=a.n_steps,
-                precision=a.precision, seed=1) as c:
+    kw = dict(mag=a.mag, action=a.action, n_stout=a.n_stout, rho=0.1, n_steps=a.n_steps, precision=a.precision,
+              seed=1)
+    if a.ensemble:
+        import numpy as np
+
+        rng = np.random.default_rng(4)
+        dims = [(8,) * 4] * 48 + [(12,) * 4] * 32 + [(16,) * 4] * 16
+        chains = [dict(dims=d, beta=float(b)) for d, b in zip(dims, rng.uniform(2.0, 2.6, len(dims)))]
+        ctx = M.Chmc(chains=chains, **kw)
+    else:
+        ctx = M.Chmc(tuple(a.dims), **kw)
+    with ctx as c:
         c.hot_start(1)
         out = {"dims": a.dims, "precision": a.precision, "n_stout": a.n_stout}
         if not a.no_tune:
@@ -59,6 +74,20 @@ def main(argv=None) -> int:
                 torch.cuda.nvtx.range_pop()
             out["traj_ms"] = c.last_run_ms() / a.traj
             out["delta_h"] = [r[0]["delta_h"] for r in recs]
+        if a.wilson:
+            import torch
+
+            c.wilson_loops(a.wilson, a.wilson)
+            torch.cuda.synchronize()
+            if a.nvtx:
+                torch.cuda.nvtx.range_push("wilson")
+            ms = []
+            for _ in range(a.reps):
+                c.wilson_loops(a.wilson, a.wilson)
+                ms.append(c.last_measure_ms())
+            if a.nvtx:
+                torch.cuda.nvtx.range_pop()
+            out["wilson_ms"] = sum(ms) / len(ms)
         for k in a.kernels:
             if a.nvtx:
                 import torch
