@@ -670,6 +670,16 @@ def run_gpu(args, params, rank, world, dist):
         line["other_configs"] = sub
     if wl:
         line["wilson_loops_ms_per_step"] = wl_ms / args.steps
+        # HBM roofline of one Wilson-loop measurement (R, T <= wl, three spatial directions): per direction
+        # the R-line planes (first: read U, write the line; then read U and the previous line, write), per T
+        # the temporal line (the same) and the accumulation pass (reads the wl S-line planes and the
+        # temporal line once per site; the shifted reads come from L2)
+        per_dir = (288 + (wl - 1) * 432) + (288 + (wl - 1) * 432) + wl * (wl + 1) * 144
+        wbytes = 3 * per_dir * V
+        wach = wbytes / (wl_ms / args.steps * 1e-3) / 1e9
+        line["wilson_hbm"] = {"achieved": wach, "peak": hbm_peak, "unit": "GB/s", "frac": wach / hbm_peak,
+                              "bytes_per_measurement": wbytes,
+                              "share_of_step": wl_ms / (ms64 if ms64 else 1.0)}
     print(json.dumps(line), flush=True)
 
 

@@ -253,6 +253,79 @@ int mag_gauge_save_nersc(mag_ctx* ctx, int chain, const char* path, int two_row,
 /* header only, no device work (computed fields are 0) */
 int mag_nersc_read_header(const char* path, mag_nersc_info* info);
 
+/* --------------------------------------------------- domain decomposition */
+/* One lattice split along x3 into nshards slabs of dims[3] / nshards time
+   slices (replaces qlat's expanded Geometry and fetch_expanded_chart,
+   field-hmc.h:777-781 and :544-558, which run_chmc and
+   force_gradient_integrator call before every force; the kinetic, plaquette
+   and rectangle sums of get_hamiltonian are added over the slabs as by its
+   MPI_Allreduce, field-hmc.h:628, and every slab takes the accept decision
+   from the same sums and uniform, as the MPI_Bcast of :823 ensures).  Each
+   slab is a context over its time slices plus `halo` slices of each
+   neighbour; the halos are refreshed wherever a kernel reads across the
+   boundary (the links of each force evaluation, every stout level, the
+   double links, each level's Lambda, and the links of the Hamiltonian's
+   smearing).  The shards live on the current device and are driven by one
+   host thread each.  Requirements: dims[3] % nshards == 0; 2 <= halo <=
+   dims[3] / nshards; dims[3] / nshards a multiple of mag (constrained
+   segments stay inside one slab); dims[0] dims[1] dims[2] a multiple of 32.
+   Results equal the undivided context's up to the order of the global sums
+   (MAG_ERR_STATE if the slabs ever disagree on the accept step). */
+typedef struct mag_dd mag_dd;
+int mag_dd_create(const mag_params* p, int nshards, int halo, mag_dd** out);
+int mag_dd_destroy(mag_dd* dd);
+/* the lattice's links / momenta in the host layout of mag_gauge_set (every slab
+   takes its slices and its halos) and back (every slab gives its own slices) */
+int mag_dd_gauge_set(mag_dd* dd, const double* host);
+int mag_dd_gauge_get(mag_dd* dd, double* host);
+int mag_dd_momentum_set(mag_dd* dd, const double* host);
+int mag_dd_momentum_get(mag_dd* dd, double* host);
+/* the Philox hot start and uniforms of the undivided lattice (site indices of the whole lattice) */
+int mag_dd_hot_start(mag_dd* dd, uint64_t seed);
+int mag_dd_uniforms_set(mag_dd* dd, const double* u);
+/* get_force (field-hmc.h:339-425) of the whole lattice, halo exchanges included */
+int mag_dd_gauge_force(mag_dd* dd, double* host_force);
+/* one run_chmc trajectory (field-hmc.h:806-843) of the whole lattice */
+int mag_dd_trajectory(mag_dd* dd, int refresh_momenta, mag_traj_result* result);
+/* the context of slab `rank` (its time slices are [rank, rank + 1) dims[3] / nshards) */
+int mag_dd_shard(mag_dd* dd, int rank, mag_ctx** ctx);
+
+/* One slab per process (or thread), the halos moved by the caller (MPI, NCCL,
+   gloo), as qlat's fetch_expanded_chart moves them through MPI.
+   mag_shard_create makes the context of slab `rank` (same requirements as
+   mag_dd_create); mag_set_halo_fn installs the callback, after which every call
+   of the context that reads across the slab boundary or forms the
+   Hamiltonian's sums (force, integration, trajectory, Hamiltonian) invokes it,
+   every slab in the same order.  Host fields passed to mag_gauge_set and the
+   like are the slab's own layout: its dims[3] / nshards + 2 halo time slices,
+   lattice time slice rank * dims[3] / nshards - halo first (periodically).
+   Trajectories run eagerly (mag_trajectory), not as captured graphs. */
+enum { MAG_HALO_EXCHANGE = 0, MAG_HALO_SUM = 1 };
+typedef struct mag_halo_op {
+    int kind;            /* MAG_HALO_EXCHANGE or MAG_HALO_SUM */
+    int rank, nshards;   /* this slab; neighbours are (rank -+ 1) mod nshards */
+    /* MAG_HALO_EXCHANGE: a device field of nplanes planes, plane p at base + p * plane_bytes.
+       In every plane send the slab_bytes at send_lo to the lower neighbour (it stores them at
+       its recv_hi) and those at send_hi to the upper neighbour (its recv_lo); receive the
+       lower neighbour's send_hi bytes at recv_lo and the upper neighbour's send_lo bytes at
+       recv_hi.  Offsets are bytes within a plane.  The field was produced by work on `stream`
+       (a cudaStream_t): order the transfers after it, and make later work on `stream` see the
+       received bytes (e.g. NCCL send/recv on `stream`, or synchronise it around host copies). */
+    void* base;
+    int nplanes;
+    size_t plane_bytes, slab_bytes, send_lo, send_hi, recv_lo, recv_hi;
+    /* MAG_HALO_SUM: replace sums[0 .. nsums) (host doubles) by their sums over all slabs and,
+       when maxval is not NULL, *maxval by its maximum over all slabs */
+    double* sums;
+    int nsums;
+    double* maxval;
+    void* stream;
+} mag_halo_op;
+/* returns 0 on success; any other value makes the calling entry point fail with MAG_ERR_STATE */
+typedef int (*mag_halo_fn)(void* user, const mag_halo_op* op);
+int mag_shard_create(const mag_params* p, int nshards, int rank, int halo, mag_ctx** out);
+int mag_set_halo_fn(mag_ctx* ctx, mag_halo_fn fn, void* user);
+
 /* ------------------------------------------------------- allocation-free */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
    (a driver that hands this library memory from a device pool it manages

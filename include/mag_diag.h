@@ -28,12 +28,23 @@ int mag_time_force(mag_ctx* ctx, int reps, double* ms_per_eval);
    word checksum), "nersc_crc" (segment CRC-32), "nersc_to_links",
    "nersc_from_links", "nersc_plaq" (plaquette and link-trace sums) */
 int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms_per_launch);
-/* re-run the launch-configuration tuner: time every register-cap variant of the
-   staple / force / stout kernels on the live fields (`reps` launches each) and
-   keep the fastest; report (may be NULL) receives a JSON object
-   {"family": [min blocks per SM for FP64, for FP32], ...}.  The first
+/* re-run the launch-configuration tuner: time every variant of the staple /
+   force / stout kernels on the live fields (`reps` launches each) and keep the
+   fastest.  Variants: one thread per link at minimum blocks per SM 2..5
+   ("t1m2".."t1m5", register caps), and for the staple, force and chain-rule
+   kernels the direction split "s<NS>r<R>" (NS = 3 or 6 warps per 32-link tile,
+   register cap R).  Every variant is timed; the choice is made among the
+   one-thread-per-link variants, which give bit-identical results (the split
+   shapes sum in another order and are selected only by mag_set_kernel_variant).
+   report (may be NULL) receives a JSON object
+   {"family": {"fp64": [chosen, {variant: ms, ...}], "fp32": [...]}, ...}
+   (times only for the families and precisions the context tuned).  The first
    trajectory, integration or graph build of a context runs the tuner once. */
 int mag_autotune(mag_ctx* ctx, int reps, char* report, size_t len);
+/* use `variant` (a name as in the mag_autotune report) for kernel `family`
+   ("force", "staple", "stout_forward", "stout_lambda", "stout_chain") at
+   precision 0 (FP64) or 1 (FP32) from now on, in place of the tuner's choice */
+int mag_set_kernel_variant(mag_ctx* ctx, const char* family, int precision, const char* variant);
 /* number of kernel nodes in the captured trajectory graph (building it if needed) */
 int mag_graph_kernel_count(mag_ctx* ctx, int* kernels);
 /* measured CUDA-core FMA throughput of this device: precision 0 = FP64 FMA,

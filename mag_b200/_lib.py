@@ -153,6 +153,7 @@ SIGNATURES = {
     "mag_time_kernel": [_CTX, ctypes.c_char_p, ctypes.c_int, _DP],
     "mag_graph_kernel_count": [_CTX, _IP],
     "mag_autotune": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.c_size_t],
+    "mag_set_kernel_variant": [_CTX, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p],
     "mag_action_sums_noalloc": [_IP, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "mag_probe_fma_peak": [ctypes.c_int, _DP],
     "mag_gauge_load_nersc": [_CTX, ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
@@ -160,6 +161,19 @@ SIGNATURES = {
                              ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
     "mag_nersc_read_header": [ctypes.c_char_p, ctypes.POINTER(NerscInfo)],
     "mag_crc32_host": [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint32)],
+    "mag_dd_create": [ctypes.POINTER(MagParams), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "mag_dd_destroy": [ctypes.c_void_p],
+    "mag_dd_gauge_set": [ctypes.c_void_p, _DP],
+    "mag_dd_gauge_get": [ctypes.c_void_p, _DP],
+    "mag_dd_momentum_set": [ctypes.c_void_p, _DP],
+    "mag_dd_momentum_get": [ctypes.c_void_p, _DP],
+    "mag_dd_hot_start": [ctypes.c_void_p, ctypes.c_uint64],
+    "mag_dd_uniforms_set": [ctypes.c_void_p, _DP],
+    "mag_dd_gauge_force": [ctypes.c_void_p, _DP],
+    "mag_dd_trajectory": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(TrajResult)],
+    "mag_dd_shard": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_CTX)],
+    "mag_shard_create": [ctypes.POINTER(MagParams), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CTX)],
+    "mag_set_halo_fn": [_CTX, ctypes.c_void_p, ctypes.c_void_p],
 }
 _RESTYPE = {"mag_last_error": ctypes.c_char_p}
 

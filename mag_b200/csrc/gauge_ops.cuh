@@ -78,6 +78,60 @@ MAG_HD mat3<T> staple_sum(const LinkPlanes<T>& U, const LinkPlanes<T>& W, const 
     return A;
 }
 
+// The part of staple_sum that belongs to one direction nu != mu, in two
+// halves for the direction-split kernels (one warp computes one half of one
+// nu for 32 links):
+//   ext : c1 [(R1 + R2) U_mu^dag(x+mu) + U_mu^dag(x-mu) (R5 + R6)]   (Iwasaki)
+//   near: c0 (P_up + P_dn) + c1 (R3 + R4)
+// The common factors U_mu^dag(x +- mu) multiply this plane's mu-extended
+// rectangles alone (two more products per plane than staple_sum, which
+// applies them once to the sums over nu).  Summed over both halves and the
+// three nu it is A.
+template <typename T, bool IWASAKI>
+MAG_HD mat3<T> staple_part_ext(const LinkPlanes<T>& U, const LinkPlanes<T>& W, const ChainInfo& ci, const Site& st,
+                               int mu, int nu) {
+    mat3<T> A;
+    if (!IWASAKI) {
+        set_zero(A);
+        return A;
+    }
+    mat3<T> t = mul_2r(U.load_rows01(nu, st.g), W.load(mu, nb(ci, st, nu, 1)));
+    mat3<T> acc = mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 2)));
+    t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), W.load(mu, nb(ci, st, nu, -1)));
+    add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 2, nu, -1))));
+    A = mul_nd(acc, U.load(mu, nb(ci, st, mu, 1)));
+    t = mul_2r(U.load_rows01(nu, nb(ci, st, mu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, 1)));
+    acc = mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1)));
+    t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, mu, -1, nu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, -1)));
+    add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
+    mul_dn_acc(A, U.load(mu, nb(ci, st, mu, -1)), acc);
+    return scaled(A, (T)ci.c1);
+}
+template <typename T, bool IWASAKI>
+MAG_HD void staple_part_near_acc(mat3<T>& A, const LinkPlanes<T>& U, const LinkPlanes<T>& W, const ChainInfo& ci,
+                                 const Site& st, int mu, int nu) {
+    const T c0 = IWASAKI ? (T)ci.c0 : T(1);
+    if (IWASAKI) {
+        const T c1 = (T)ci.c1;
+        mat3<T> t = mul_2r(W.load_rows01(nu, st.g), U.load(mu, nb(ci, st, nu, 2)));
+        axpy(A, c1, mul_nd_su3(t, W.load(nu, nb(ci, st, mu, 1))));
+        t = mul_dn_2r(W.load_cols01(nu, nb(ci, st, nu, -2)), U.load(mu, nb(ci, st, nu, -2)));
+        axpy(A, c1, mul_su3(t, W.load(nu, nb(ci, st, mu, 1, nu, -2))));
+    }
+    mat3<T> t = mul_2r(U.load_rows01(nu, st.g), U.load(mu, nb(ci, st, nu, 1)));
+    axpy(A, c0, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
+    t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), U.load(mu, nb(ci, st, nu, -1)));
+    axpy(A, c0, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
+}
+// both halves of one nu
+template <typename T, bool IWASAKI>
+MAG_HD mat3<T> staple_part(const LinkPlanes<T>& U, const LinkPlanes<T>& W, const ChainInfo& ci, const Site& st,
+                           int mu, int nu) {
+    mat3<T> A = staple_part_ext<T, IWASAKI>(U, W, ci, st, mu, nu);
+    staple_part_near_acc<T, IWASAKI>(A, U, W, ci, st, mu, nu);
+    return A;
+}
+
 // Plaquette staple sum (the stout "stp", field-multi.h:34 with thin staples):
 // sum_nu U_nu(x)U_mu(x+nu)U_nu^dag(x+mu) + U_nu^dag(x-nu)U_mu(x-nu)U_nu(x-nu+mu)
 template <typename T>
@@ -146,6 +200,42 @@ MAG_HD mat3<T> stout_chain(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, cons
     mat3<T> z = Zp.load(mu, st.g);  // Z' e^{iQ}
     add_to(z, times_i(t, (T)ci.rho));
     return z;
+}
+
+// The bracket of stout_chain for one direction nu != mu, in two halves for
+// the direction-split kernels: the upper staple's terms (upper) and the lower
+// staple's (lower_acc adds them to t).  Summed over both halves and the three
+// nu and multiplied by i rho it is Z - Z' e^{iQ}.
+template <typename T>
+MAG_HD mat3<T> stout_chain_upper(const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, const herm8<T>& lx,
+                                 const ChainInfo& ci, const Site& st, int mu, int nu) {
+    const mat3<T> unx = U.load(nu, st.g);
+    const mat3<T> D = mul_nd_su3(U.load_rows01(nu, nb(ci, st, mu, 1)), U.load(mu, nb(ci, st, nu, 1)));
+    const mat3<T> E = mul_nd_su3(D, unx);
+    mat3<T> t = mul_hm(Lam.load(nu, nb(ci, st, mu, 1)), E);
+    herm8<T> dl = Lam.load(nu, st.g);
+#pragma unroll
+    for (int k = 0; k < 8; k++) dl.h[k] = lx.h[k] - dl.h[k];
+    mat3<T> inner = mul_dn_mh(unx, dl);
+    mul_hm_nd_sub(inner, Lam.load(mu, nb(ci, st, nu, 1)), unx);
+    mul_acc(t, D, inner);
+    return t;
+}
+template <typename T>
+MAG_HD void stout_chain_lower_acc(mat3<T>& t, const LinkPlanes<T>& U, const AlgPlanes<T>& Lam, const herm8<T>& lx,
+                                  const ChainInfo& ci, const Site& st, int mu, int nu) {
+    const int gm = nb(ci, st, nu, -1);
+    const mat3<T> umn = U.load(mu, gm);
+    const mat3<T> unn = U.load(nu, gm);
+    const mat3<T> G = mul_dn_su3(umn, unn);
+    herm8<T> dl = Lam.load(mu, gm);
+    const herm8<T> ln = Lam.load(nu, gm);
+#pragma unroll
+    for (int k = 0; k < 8; k++) dl.h[k] -= ln.h[k];
+    mat3<T> inner = mul_mh(G, lx);
+    mul_sub(inner, mul_dn_mh(umn, dl), unn);
+    mul_hm_sub(inner, Lam.load(nu, nb(ci, st, mu, 1, nu, -1)), G);
+    mul_dn_acc(t, U.load(nu, nb(ci, st, mu, 1, nu, -1)), inner);
 }
 
 // Lambda of compute_Lambda (field-multi.h:180-269) and Z' exp(iQ) for one link.
@@ -218,30 +308,25 @@ MAG_HD void stout_lambda(const herm8<T>& q, const mat3<T>& Z, const mat3<T>& Ul,
 
 // Link update of evolve_gauge_field (field-hmc.h:442-482) with X = momentum or
 // force and step eps:  0: e^{i eps X(x)} U;  1: e^{i eps X(x-mu)} U e^{-i eps X(x)};
-// 10: U e^{-i eps X(x)};  100: e^{i eps X(x-mu)} U.
+// 10: U e^{-i eps X(x)};  100: e^{i eps X(x-mu)} U.  One exponential per link
+// (two for the interior links of a segment, case 1, which only mag >= 3 has),
+// evaluated at one call site in a loop so that it is inlined once.
 template <typename TU, typename TX>
 MAG_HD mat3<TU> evolve_link(const mat3<TU>& u, const AlgPlanes<TX>& X, double eps, int ccase, int g, int gm, int mu) {
     mat3<TU> r = u;
-    if (ccase == 1 || ccase == 100) {
-        herm8<TX> xl = X.load(mu, gm);
+    const int nexp = ccase == 1 ? 2 : 1;
+#pragma unroll 1
+    for (int k = 0; k < nexp; k++) {
+        // left factor e^{i eps X(y)} (cases 0, 100, and 1 first) or right factor e^{-i eps X(x)} (10, 1 second)
+        const bool right = ccase == 10 || k == 1;
+        const int y = (ccase == 100 || (ccase == 1 && k == 0)) ? gm : g;
+        const herm8<TX> xl = X.load(mu, y);
+        const TU s = (TU)(right ? -eps : eps);
         herm8<TU> q;
 #pragma unroll
-        for (int k = 0; k < 8; k++) q.h[k] = (TU)xl.h[k] * (TU)eps;
-        r = mul(expiQ(q), r);
-    }
-    if (ccase == 0) {
-        herm8<TX> xl = X.load(mu, g);
-        herm8<TU> q;
-#pragma unroll
-        for (int k = 0; k < 8; k++) q.h[k] = (TU)xl.h[k] * (TU)eps;
-        r = mul(expiQ(q), r);
-    }
-    if (ccase == 1 || ccase == 10) {
-        herm8<TX> xl = X.load(mu, g);
-        herm8<TU> q;
-#pragma unroll
-        for (int k = 0; k < 8; k++) q.h[k] = (TU)xl.h[k] * (TU)(-eps);
-        r = mul(r, expiQ(q));
+        for (int j = 0; j < 8; j++) q.h[j] = (TU)xl.h[j] * s;
+        const mat3<TU> e = expiQ(q);
+        r = right ? mul(r, e) : mul(e, r);
     }
     return r;
 }

@@ -64,7 +64,8 @@ struct AcceptArgs {
 // ---- force and staples (kernels_force.cu)
 // `v` selects the register-cap variant 0..3 (minimum 2..5 resident 128-thread
 // blocks per SM, i.e. at most 255 / 168 / 128 / 102 registers per thread).
-constexpr int kNumVariants = 4;
+constexpr int kNumRegVariants = 4;  // one thread per link, register caps (minimum blocks per SM 2..5)
+constexpr int kNumVariants = 9;     // + direction split: 3 or 6 warps per 32-link tile, register caps
 enum KernelFamily { KF_FORCE = 0, KF_STAPLE, KF_STOUT_FWD, KF_STOUT_LAMBDA, KF_STOUT_CHAIN, KF_COUNT };
 
 // W = double links U(x,mu) U(x+mu,mu); the Iwasaki staple kernels read W of the same field

@@ -129,7 +129,7 @@ __global__ void k_reunitarize(DevGeom g, LinkPlanes<double> U, LinkPlanes<float>
                 const double dr = m.e[i][j].re - old.e[i][j].re, di = m.e[i][j].im - old.e[i][j].im;
                 s += dr * dr + di * di;
             }
-        dev = sqrt(s);
+        dev = interior(ci, st) ? sqrt(s) : 0.0;  // a shard's halo links are not its own
         U.store(mu, st.g, m);
         if (Ucopy.p) Ucopy.store(mu, st.g, convert<float>(m));
     }
@@ -184,7 +184,7 @@ __global__ void k_action_partials(DevGeom g, LinkPlanes<T> U, int with_rect, dd2
     ChainInfo ci;
     Site st;
     dd2 p = {0.0, 0.0}, r = {0.0, 0.0};
-    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st)) {
+    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st) && interior(ci, st)) {
         p.hi = site_plaquette(U, ci, st);
         if (with_rect) r.hi = site_rectangle(U, ci, st);
     }
@@ -201,7 +201,7 @@ __global__ void k_kinetic_partials(DevGeom g, AlgPlanes<double> P, dd2* partial)
     ChainInfo ci;
     Site st;
     dd2 k = {0.0, 0.0};
-    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st)) {
+    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st) && interior(ci, st)) {
         double acc = 0.0;
 #pragma unroll
         for (int mu = 0; mu < 4; mu++) {
@@ -220,7 +220,7 @@ __global__ void k_link_trace_partials(DevGeom g, LinkPlanes<double> U, dd2* part
     ChainInfo ci;
     Site st;
     dd2 k = {0.0, 0.0};
-    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st)) {
+    if (locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st) && interior(ci, st)) {
         double acc = 0.0;
 #pragma unroll
         for (int mu = 0; mu < 4; mu++) acc += retr(U.load(mu, st.g));
@@ -306,7 +306,7 @@ __global__ void k_record_plaquette(DevGeom g, const dd2* sums, TrajRecord* rec, 
     const long long slot = *traj_counter - *hist_base;
     for (int c = threadIdx.x; c < g.nchain; c += blockDim.x) {
         const ChainInfo ci = g.chains[c];
-        rec[c].avg_plaquette = dd_val(sums[c * NUM_SLOTS + SLOT_PLAQ_THIN]) / (18.0 * ci.V);
+        rec[c].avg_plaquette = dd_val(sums[c * NUM_SLOTS + SLOT_PLAQ_THIN]) / (18.0 * ci.Vg);
         if (hist && slot >= 0 && slot < hist_cap) hist[slot * g.nchain + c] = rec[c];
     }
     __syncthreads();
@@ -322,7 +322,7 @@ __global__ void k_momenta(DevGeom g, AlgPlanes<double> P, unsigned long long see
     if (!locate(g, gs, ci, st)) return;
     const int mu = blockIdx.y;
     const int chain = g.c2c[gs / MAG_CHUNK];
-    const uint32_t link = (uint32_t)(4 * st.s + mu);
+    const uint32_t link = (uint32_t)(4 * lattice_site(ci, st) + mu);
     const uint32_t traj = (uint32_t)(*traj_counter);
     double xi[8];
     const unsigned long long key = seed + g.stream_index[chain];
@@ -348,7 +348,7 @@ __global__ void k_hot_start(DevGeom g, LinkPlanes<double> U, unsigned long long 
     if (!locate(g, gs, ci, st)) return;
     const int mu = blockIdx.y;
     const int chain = g.c2c[gs / MAG_CHUNK];
-    const uint32_t link = (uint32_t)(4 * st.s + mu);
+    const uint32_t link = (uint32_t)(4 * lattice_site(ci, st) + mu);
     double x[12];
     const unsigned long long key = seed + g.stream_index[chain];
     for (int j = 0; j < 3; j++) gauss4(key, link, (uint32_t)j, 0u, RNG_HOT, x + 4 * j);

@@ -71,29 +71,52 @@ __global__ void k_line_extend(DevGeom g, LinkPlanes<double> U, int d, LinkPlanes
     out.store(0, st.g, prev.p ? mul(prev.load(0, st.g), u) : u);
 }
 
-// partial[block * Rmax + R-1] = sum_x ReTr W_i(R, T)(x)
-__global__ void k_wloop_accum(DevGeom g, LinkPlanes<double> lines, int Rmax, LinkPlanes<double> tl, int i, int T,
-                              dd2* partial) {
+// partial[block * Rmax + R-1] = sum_x ReTr W_i(R, T)(x).  The R values are
+// taken four at a time: a thread forms its site's four loops (their loads
+// issued together) and the block reduces the four sums at once, instead of one
+// block reduction (two barriers) per R.  ReTr(S_R(x) T(x+Ri) S_R(x+Tt)^dag
+// T(x)^dag) = ReTr(a c^dag) with a = S_R(x) T(x+Ri), c = T(x) S_R(x+Tt): two
+// products and one trace of a product per loop.
+constexpr int kRChunk = 4;
+__global__ void __launch_bounds__(kBlock, 2) k_wloop_accum(DevGeom g, LinkPlanes<double> lines, int Rmax,
+                                                           LinkPlanes<double> tl, int i, int T, dd2* partial) {
+    __shared__ dd2 sm[kBlock / 32][kRChunk];
     ChainInfo ci;
     Site st;
     const bool ok = locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st);
-    mat3<double> tx, sT;
-    int gT = 0;
+    int gT = 0, gR = 0;
     if (ok) {
-        tx = tl.load(0, st.g);
         gT = st.g + wrap_shift(ci, st.x[3], 3, T);
+        gR = st.x[i];
     }
-    for (int R = 1; R <= Rmax; R++) {
-        dd2 v{0.0, 0.0};
-        if (ok) {
-            const LinkPlanes<double> S{lines.p + (size_t)(R - 1) * 9 * lines.vpad, lines.vpad};
-            const mat3<double> a = mul(S.load(0, st.g), tl.load(0, st.g + wrap_shift(ci, st.x[i], i, R)));
-            sT = S.load(0, gT);
-            const mat3<double> b = mul_nd(a, sT);       // S_R(x) T(x+Ri) S_R(x+Tt)^dag
-            v.hi = retr(mul_nd(b, tx));                  // ... T(x)^dag
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int R0 = 1; R0 <= Rmax; R0 += kRChunk) {
+        double v[kRChunk];
+#pragma unroll
+        for (int r = 0; r < kRChunk; r++) {
+            const int R = R0 + r;
+            v[r] = 0.0;
+            if (ok && R <= Rmax) {
+                const LinkPlanes<double> S{lines.p + (size_t)(R - 1) * 9 * lines.vpad, lines.vpad};
+                const mat3<double> a = mul(S.load(0, st.g), tl.load(0, st.g + wrap_shift(ci, gR, i, R)));
+                const mat3<double> c = mul(tl.load(0, st.g), S.load(0, gT));
+                v[r] = retr_mul_nd(a, c);
+            }
         }
-        v = block_reduce(v);
-        if (threadIdx.x == 0) partial[(size_t)blockIdx.x * Rmax + (R - 1)] = v;
+#pragma unroll
+        for (int r = 0; r < kRChunk; r++)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v[r] += __shfl_down_sync(0xffffffffu, v[r], o);
+        __syncthreads();  // the previous chunk's sums have been read
+        if (lane == 0)
+#pragma unroll
+            for (int r = 0; r < kRChunk; r++) sm[wid][r] = dd2{v[r], 0.0};
+        __syncthreads();
+        if (threadIdx.x < kRChunk && R0 + (int)threadIdx.x <= Rmax) {
+            dd2 s = sm[0][threadIdx.x];
+            for (int w = 1; w < kBlock / 32; w++) s = dd_add(s, sm[w][threadIdx.x]);
+            partial[(size_t)blockIdx.x * Rmax + R0 - 1 + threadIdx.x] = s;
+        }
     }
 }
 

@@ -29,7 +29,12 @@ struct ChainInfo {
     int V;       // sites of this chain
     int off;     // first global site
     int mag;     // constraint magnification (0: free)
-    int pad;
+    // A shard of a lattice decomposed along x3 holds local x3 in [0, L[3]):
+    // the interior [lo3, hi3) and halo slabs on both sides.  Local x3 = 0 is
+    // lattice coordinate org3 (mod L3g); Vg counts the whole lattice's sites.
+    // An undivided chain has org3 = 0, L3g = L[3], lo3 = 0, hi3 = L[3], Vg = V.
+    int org3, L3g, lo3, hi3;
+    int Vg;
     double beta, c0, c1, rho;
 };
 
@@ -65,16 +70,30 @@ MAG_HD int nb(const ChainInfo& ci, const Site& st, int d1, int k1, int d2, int k
     return st.g + shift_off(ci, st.x[d1], d1, k1) + shift_off(ci, st.x[d2], d2, k2);
 }
 
+// lattice coordinate x3 of local x3 (a shard's halo and interior), and
+// whether a site belongs to the chain's own (interior) sites
+MAG_HD int x3_lattice(const ChainInfo& ci, int x3) {
+    int w = (x3 + ci.org3) % ci.L3g;
+    return w < 0 ? w + ci.L3g : w;
+}
+MAG_HD bool interior(const ChainInfo& ci, const Site& st) { return st.x[3] >= ci.lo3 && st.x[3] < ci.hi3; }
+// site index in the whole lattice (x0 fastest); the local index for an undivided chain
+MAG_HD long lattice_site(const ChainInfo& ci, const Site& st) {
+    return st.x[0] + (long)ci.L[0] * (st.x[1] + (long)ci.L[1] * (st.x[2] + (long)ci.L[2] * x3_lattice(ci, st.x[3])));
+}
+
 // is_constrained (field-hmc.h:309-337): 0 free, 1 interior, 10 first, 100 last
+// (lattice coordinates, so that a shard classifies its halo as the lattice does)
 MAG_HD int constraint_case(const ChainInfo& ci, const Site& st, int mu) {
     const int m = ci.mag;
     if (!m) return 0;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         if (i == mu) continue;
-        if (st.x[i] % m != 0) return 0;
+        const int xi = i == 3 ? x3_lattice(ci, st.x[3]) : st.x[i];
+        if (xi % m != 0) return 0;
     }
-    const int r = st.x[mu] % m;
+    const int r = (mu == 3 ? x3_lattice(ci, st.x[3]) : st.x[mu]) % m;
     if (r == m - 1) return 100;
     if (r == 0) return 10;
     return 1;

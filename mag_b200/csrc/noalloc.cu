@@ -192,6 +192,8 @@ extern "C" int mag_action_sums_noalloc(const int dims[4], const double* d_links,
                                             "-site limit of its static scratch; use mag_action");
     }
     ci.V = (int)V;
+    ci.L3g = ci.hi3 = ci.L[3];
+    ci.Vg = (int)V;
     dd2* partials = nullptr;
     const int r = partials_for_current_device(&partials);
     if (r != MAG_OK) return r;

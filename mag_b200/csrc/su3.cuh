@@ -266,6 +266,19 @@ MAG_HD T retr_mul(const mat3<T>& a, const mat3<T>& b) {
         }
     return s;
 }
+// Re Tr(a * b^dag) = sum_ij Re(a_ij conj(b_ij)) without forming the product
+template <typename T>
+MAG_HD T retr_mul_nd(const mat3<T>& a, const mat3<T>& b) {
+    T s = T(0);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            s = fmaT(a.e[i][j].re, b.e[i][j].re, s);
+            s = fmaT(a.e[i][j].im, b.e[i][j].im, s);
+        }
+    return s;
+}
 // Tr(a * b)
 template <typename T>
 MAG_HD cplx<T> tr_mul(const mat3<T>& a, const mat3<T>& b) {
@@ -679,6 +692,58 @@ MAG_HD ch_coef_f ch_to_float(const ch_coef& c) {
     return r;
 }
 
+// exp(iQ)'s coefficients f_j alone, in double, by the same series as
+// ch_series: f_j = sum_n i^n/n! (a_n, b_n, d_n)_j with Q^n = a_n + b_n Q + d_n Q^2.
+// The terms are unrolled in (odd, even) pairs with 1/n folded to constants;
+// with q = sqrt(4 c1 / 3) >= every eigenvalue modulus, a_n, b_n, d_n are
+// bounded by q^n (q >= 1) or q^(n-2) (q < 1), so the sum stops once
+// q^n / n! (or q^(n-2) / n!) falls below 1e-17: about 10 terms for the
+// exponents of a link update (q ~ 0.1), 16 for a stout level (q ~ 0.5).
+// No transcendental function is evaluated.  exp(iQ) from these f_j agrees
+// with exp(iQ) from the closed form to rounding (a long-double Taylor check:
+// <= 3e-15 for Q entries of scale 1e-4 to 2, against the closed form's
+// <= 6e-16 to 3e-15): the closed form's own f_j lose accuracy at small Q
+// (|df| ~ 1e-12 at scale 0.01), but those errors reach exp(iQ) multiplied by
+// Q and Q^2.  The derivative coefficients b_ij of compute_Lambda have no such
+// damping, which is why the FP64 Lambda keeps the reference's closed form
+// (same numbers as the reference, errors included).  Returns false for q > 3.
+MAG_HD bool ch_series_exp_d(double c0, double c1, double f[6]) {
+    const double q2 = (4.0 / 3.0) * c1;
+    if (q2 > 9.0) return false;
+    const double q = sqrt(q2);
+    const bool qbig = q >= 1.0;
+    double a = 1.0, b = 0.0, d = 0.0;
+    double f0r = 1.0, f1r = 0.0, f2r = 0.0, f0i = 0.0, f1i = 0.0, f2i = 0.0;
+    double coef = 1.0, bound = 1.0;
+#pragma unroll
+    for (int n = 1; n < 40; n += 2) {
+        {  // odd term: i^n = (-1)^((n-1)/2) i
+            const double na = c0 * d, nb = fmaT(c1, d, a), nd = b;
+            a = na; b = nb; d = nd;
+            coef *= 1.0 / n;
+            bound *= (qbig || n > 2 ? q : 1.0) * (1.0 / n);
+            const double sg = ((n >> 1) & 1) ? -coef : coef;
+            f0i = fmaT(sg, a, f0i);
+            f1i = fmaT(sg, b, f1i);
+            f2i = fmaT(sg, d, f2i);
+        }
+        {  // even term n + 1: i^(n+1) = (-1)^((n+1)/2)
+            const int m = n + 1;
+            const double na = c0 * d, nb = fmaT(c1, d, a), nd = b;
+            a = na; b = nb; d = nd;
+            coef *= 1.0 / m;
+            bound *= (qbig || m > 2 ? q : 1.0) * (1.0 / m);
+            const double sg = ((m >> 1) & 1) ? -coef : coef;
+            f0r = fmaT(sg, a, f0r);
+            f1r = fmaT(sg, b, f1r);
+            f2r = fmaT(sg, d, f2r);
+        }
+        if (n + 1 >= 4 && bound < 1e-17) break;
+    }
+    f[0] = f0r; f[1] = f0i; f[2] = f1r; f[3] = f1i; f[4] = f2r; f[5] = f2i;
+    return true;
+}
+
 // Q^2 of a compact Hermitian traceless matrix (Hermitian result)
 template <typename T>
 MAG_HD mat3<T> herm_square(const herm8<T>& q) {
@@ -747,11 +812,18 @@ MAG_HD mat3<T> expiQ(const herm8<T>& q) {
     } else {
         double c0, c1;
         ch_invariants(Q, QQ, c0, c1);
-        const ch_coef c = ch_coefficients<false>(c0, c1);
-        if (c.trivial) return unit_mat<T>();
-        f0 = mk<T>((T)c.f0r, (T)c.f0i);
-        f1 = mk<T>((T)c.f1r, (T)c.f1i);
-        f2 = mk<T>((T)c.f2r, (T)c.f2i);
+        if (c1 == 0.0) return unit_mat<T>();  // the reference's c1 = 0 branch (field-hmc.h:95)
+        double fs[6];
+        if (ch_series_exp_d(c0, c1, fs)) {
+            f0 = mk<T>(fs[0], fs[1]);
+            f1 = mk<T>(fs[2], fs[3]);
+            f2 = mk<T>(fs[4], fs[5]);
+        } else {
+            const ch_coef c = ch_coefficients<false>(c0, c1);
+            f0 = mk<T>((T)c.f0r, (T)c.f0i);
+            f1 = mk<T>((T)c.f1r, (T)c.f1i);
+            f2 = mk<T>((T)c.f2r, (T)c.f2i);
+        }
     }
     mat3<T> r;
 #pragma unroll

@@ -340,12 +340,18 @@ class Chmc:
         return v.value
 
     def autotune(self, reps: int = 3) -> dict:
-        """Re-run the register-cap tuner; returns {family: [minB FP64, minB FP32]}."""
+        """Re-run the launch-configuration tuner; returns
+        {family: {"fp64": [chosen variant, {variant: ms}], "fp32": [...]}}."""
         import json
 
-        buf = ctypes.create_string_buffer(1024)
+        buf = ctypes.create_string_buffer(16384)
         check(self._lib.mag_autotune(self._h, int(reps), buf, len(buf)), "mag_autotune")
         return json.loads(buf.value.decode())
+
+    def set_kernel_variant(self, family: str, precision: str, variant: str) -> None:
+        """Use `variant` (e.g. "t1m3", "s6r128") for `family` at "fp64" or "fp32" in place of the tuner's choice."""
+        check(self._lib.mag_set_kernel_variant(self._h, family.encode(), 0 if precision == "fp64" else 1,
+                                               variant.encode()), "mag_set_kernel_variant")
 
     def graph_kernel_count(self) -> int:
         v = ctypes.c_int()

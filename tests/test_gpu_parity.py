@@ -500,3 +500,25 @@ def test_gpu_force_is_minus_gpu_action_derivative(n_stout, mag, pair):
     an = -np.trace(X @ F[site, mu]).real
     assert abs(fd - an) < 2e-7 * max(1.0, abs(an)), (fd, an)
 
+
+
+VARIANTS = ["t1m2", "t1m3", "t1m4", "t1m5", "s3r168", "s3r128", "s6r168", "s6r128", "s6r96"]
+
+
+@pytest.mark.parametrize("dims,action,mag,n_stout,family", [
+    ((4, 4, 4, 6), "iwasaki", 2, 0, "force"), ((5, 3, 3, 4), "wilson", 0, 0, "force"),
+    ((4, 4, 4, 6), "iwasaki", 2, 3, "staple"), ((4, 4, 4, 6), "iwasaki", 2, 3, "stout_chain"),
+    ((5, 3, 3, 4), "iwasaki", 0, 1, "staple"), ((5, 3, 3, 4), "iwasaki", 0, 1, "stout_chain")])
+def test_every_kernel_variant_matches_the_oracle(dims, action, mag, n_stout, family):
+    """Each launch shape of the tuner (one thread per link at four register caps; the direction
+    split with 3 or 6 warps per 32-link tile at three caps) gives the force the oracle gives:
+    FP64 to 1e-11, FP32 (mixed) to 5e-5; 5 x 3 x 3 x 4 has a partial last tile."""
+    U = O.gen_hot(dims, 19)
+    po = O.make_params(dims, mag=mag, action=1 if action == "iwasaki" else 0, n_stout=n_stout, rho=0.1)
+    Fo = O.force(po, U)
+    for prec, tol in (("fp64", 1e-11), ("mixed", 5e-5)):
+        with M.Chmc(dims, mag=mag, action=action, n_stout=n_stout, rho=0.1, precision=prec) as c:
+            c.set_gauge(U)
+            for v in VARIANTS:
+                c.set_kernel_variant(family, "fp64" if prec == "fp64" else "fp32", v)
+                assert maxrel(c.get_force(), Fo) < tol, (prec, v)
