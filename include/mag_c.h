@@ -326,6 +326,35 @@ typedef int (*mag_halo_fn)(void* user, const mag_halo_op* op);
 int mag_shard_create(const mag_params* p, int nshards, int rank, int halo, mag_ctx** out);
 int mag_set_halo_fn(mag_ctx* ctx, mag_halo_fn fn, void* user);
 
+/* ---------------------------------------------------- two-level coupling */
+/* run_hmc_multi (field-multi.h:758-900): a fine lattice (dims of `fine`, all
+   even) and a coarse lattice of half the extent in every direction, coupled
+   through the stout-smeared blocked links of the fine field:
+     H = K_fine + K_coarse + S_gauge(fine)
+         - 1/eta_sqr sum_{coarse x, mu} ReTr(C(x,mu)^dag e^{iQ(2x,mu)} V(2x,mu)),
+     V(y,mu) = U(y,mu) U(y+mu,mu) (get_U), Q = -i rho TA(stp V^dag) with stp the
+     staple of the 2-link (get_Q, get_staple_rect, field-hmc.h:244-258).
+   Forces: get_Fforce (field-multi.h:409-656) and get_Cforce (:659-683); one
+   force-gradient trajectory moves both fields (force_gradient_integrator_multi,
+   :685-756).  The reference reads rho and eta_sqr from globals that are not in
+   its tree; here they are arguments.  Both fields are unconstrained (mag is
+   ignored), FP64, no stout levels of the fine action itself.  Fields cross in
+   the host layout of mag_gauge_set, fine then coarse. */
+typedef struct mag_multi mag_multi;
+int mag_multi_create(const mag_params* fine, double rho, double eta_sqr, mag_multi** out);
+int mag_multi_destroy(mag_multi* m);
+int mag_multi_gauge_set(mag_multi* m, const double* fine, const double* coarse);
+int mag_multi_gauge_get(mag_multi* m, double* fine, double* coarse);
+int mag_multi_momentum_set(mag_multi* m, const double* fine, const double* coarse);
+/* fine force (gauge + coupling) and coarse force of the current fields */
+int mag_multi_forces(mag_multi* m, double* fine_force, double* coarse_force);
+/* out = {H, kinetic energy of both levels, fine gauge action, coupling energy} */
+int mag_multi_hamiltonian(mag_multi* m, double out[4]);
+/* one trajectory from the momenta set by mag_multi_momentum_set: Metropolis with
+   `uniform` (accepted whatever Delta H while traj_index < n_forced_accept);
+   out = {H_old, H_new, Delta H, accept, reunitarisation deviation fine, coarse} */
+int mag_multi_trajectory(mag_multi* m, int traj_index, double uniform, double out[6]);
+
 /* ------------------------------------------------------- allocation-free */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
    (a driver that hands this library memory from a device pool it manages

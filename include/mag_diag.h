@@ -36,8 +36,12 @@ int mag_time_kernel(mag_ctx* ctx, const char* which, int reps, double* ms_per_la
    register cap R).  Every variant is timed; the choice is made among the
    one-thread-per-link variants, which give bit-identical results (the split
    shapes sum in another order and are selected only by mag_set_kernel_variant).
+   The tuner then times whole force evaluations with the link kernels' blocks
+   visiting a single lattice in raster order or in 2 x 2 / 4 x 4 tiles of
+   (x2, x3) rows (same results, other L2 reuse) and keeps the fastest order.
    report (may be NULL) receives a JSON object
-   {"family": {"fp64": [chosen, {variant: ms, ...}], "fp32": [...]}, ...}
+   {"family": {"fp64": [chosen, {variant: ms, ...}], "fp32": [...]}, ...,
+    "block_order": [tile, {"raster": ms, "tile2": ms, "tile4": ms}]}
    (times only for the families and precisions the context tuned).  The first
    trajectory, integration or graph build of a context runs the tuner once. */
 int mag_autotune(mag_ctx* ctx, int reps, char* report, size_t len);

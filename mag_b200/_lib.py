@@ -174,6 +174,14 @@ SIGNATURES = {
     "mag_dd_shard": [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_CTX)],
     "mag_shard_create": [ctypes.POINTER(MagParams), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_CTX)],
     "mag_set_halo_fn": [_CTX, ctypes.c_void_p, ctypes.c_void_p],
+    "mag_multi_create": [ctypes.POINTER(MagParams), ctypes.c_double, ctypes.c_double, ctypes.POINTER(ctypes.c_void_p)],
+    "mag_multi_destroy": [ctypes.c_void_p],
+    "mag_multi_gauge_set": [ctypes.c_void_p, _DP, _DP],
+    "mag_multi_gauge_get": [ctypes.c_void_p, _DP, _DP],
+    "mag_multi_momentum_set": [ctypes.c_void_p, _DP, _DP],
+    "mag_multi_forces": [ctypes.c_void_p, _DP, _DP],
+    "mag_multi_hamiltonian": [ctypes.c_void_p, _DP],
+    "mag_multi_trajectory": [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, _DP],
 }
 _RESTYPE = {"mag_last_error": ctypes.c_char_p}
 

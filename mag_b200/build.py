@@ -16,7 +16,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmag_b200.so")
-SOURCES = ["kernels_force.cu", "kernels_update.cu", "kernels_wloop.cu", "kernels_nersc.cu", "kernels_demon.cu", "kernels_matrix.cu", "mag_api.cu",
+SOURCES = ["kernels_force.cu", "kernels_update.cu", "kernels_wloop.cu", "kernels_nersc.cu", "kernels_demon.cu", "kernels_matrix.cu", "kernels_multi.cu", "mag_api.cu",
            "noalloc.cu",
            "nersc_host.cpp"]
 HEADERS = ["su3.cuh", "lattice.cuh", "gauge_ops.cuh", "rng.cuh", "kernels.h", "nersc_host.h"]

@@ -22,6 +22,11 @@ struct DevGeom {
     // key (default: the chain's position in the context; a sharded ensemble sets the
     // chain's position in the whole ensemble)
     const unsigned long long* stream_index;
+    // Order in which the link kernels' 128-site blocks visit a single lattice:
+    // tile = 0 raster (x0 fastest); tile = T > 0: the (x2, x3) rows in T x T
+    // tiles, rows of `gpr` blocks (x0 x1 = 128 gpr sites), L2 rows along x2.
+    // Only the order changes: every link is computed as in raster order.
+    int tile, gpr, L2;
 };
 
 // Per-trajectory record kept on the device, one per chain per trajectory.
@@ -64,6 +69,7 @@ struct AcceptArgs {
 // ---- force and staples (kernels_force.cu)
 // `v` selects the register-cap variant 0..3 (minimum 2..5 resident 128-thread
 // blocks per SM, i.e. at most 255 / 168 / 128 / 102 registers per thread).
+constexpr int kForceBlockSites = 128;  // sites per block of the one-thread-per-link kernels
 constexpr int kNumRegVariants = 4;  // one thread per link, register caps (minimum blocks per SM 2..5)
 constexpr int kNumVariants = 9;     // + direction split: 3 or 6 warps per 32-link tile, register caps
 enum KernelFamily { KF_FORCE = 0, KF_STAPLE, KF_STOUT_FWD, KF_STOUT_LAMBDA, KF_STOUT_CHAIN, KF_COUNT };
@@ -207,5 +213,15 @@ void launch_wilson_planar(const DevGeom& g, LinkPlanes<double> U, int Rmax, int 
 // -1 ends a shorter path; out[c]
 void launch_wilson_general(const DevGeom& g, LinkPlanes<double> U, const int* dirs, int npath, int plen,
                            int coarse_mag, dd2* partial, dd2* out, cudaStream_t s);
+
+// ---- two-level coupling (kernels_multi.cu), FP64; cf / cc the fine and coarse chain (one each, off 0).
+// Coarse links: energy density ReTr(C^dag e^{iQ} V) reduced into *energy (partial: 4 * ceil(Vc / 128)
+// dd2; both may be null), the coarse force into Fc, Lambda and C^dag e^{iQ} into Lam / Zp (each may be null).
+void launch_multi_coarse(const ChainInfo& cf, const ChainInfo& cc, LinkPlanes<double> U, LinkPlanes<double> C,
+                         double rho, double eta_sqr, AlgPlanes<double> Fc, AlgPlanes<double> Lam, LinkPlanes<double> Zp,
+                         dd2* partial, dd2* energy, cudaStream_t s);
+// F += the coupling's derivative with respect to the fine links (needs Lam, Zp of the same fields)
+void launch_multi_fine(const ChainInfo& cf, const ChainInfo& cc, LinkPlanes<double> U, AlgPlanes<double> Lam,
+                       LinkPlanes<double> Zp, double rho, double eta_sqr, AlgPlanes<double> F, cudaStream_t s);
 
 }  // namespace magb

@@ -21,11 +21,21 @@ namespace magb {
 
 namespace {
 
-constexpr int kForceBlock = 128;
+constexpr int kForceBlock = kForceBlockSites;
+
+// first site of link block b (the block's 128 sites are consecutive); see DevGeom::tile
+__device__ __forceinline__ int block_site(const DevGeom& g, int b) {
+    if (!g.tile) return b * kForceBlock;
+    const int T = g.tile, r = b / g.gpr, grp = b - r * g.gpr;
+    const int tid = r / (T * T), w = r - tid * (T * T);
+    const int tpr = g.L2 / T;  // tiles along x2
+    const int x2 = (tid % tpr) * T + w % T, x3 = (tid / tpr) * T + w / T;
+    return ((x3 * g.L2 + x2) * g.gpr + grp) * kForceBlock;
+}
 
 __device__ __forceinline__ bool locate_link(const DevGeom& g, ChainInfo& ci, Site& st, int& mu) {
     mu = blockIdx.x & 3;
-    const int gs = (blockIdx.x >> 2) * kForceBlock + threadIdx.x;
+    const int gs = block_site(g, blockIdx.x >> 2) + threadIdx.x;
     if (gs >= g.vpad) return false;
     ci = g.chains[g.c2c[gs / MAG_CHUNK]];
     const int s = gs - ci.off;

@@ -36,6 +36,9 @@ def main(argv=None) -> int:
     ap.add_argument("--ensemble", action="store_true",
                     help="the 96-chain ensemble (48 x 8^4, 32 x 12^4, 16 x 16^4, beta ~ U[2.0, 2.6) from seed 4) "
                          "in place of --dims")
+    ap.add_argument("--dd", type=int, default=0, metavar="NSHARDS",
+                    help="also time whole trajectories (wall clock, eager) of the lattice split into NSHARDS slabs "
+                         "along x3 (halo 2) next to the undivided context's eager trajectories")
     ap.add_argument("--traj", type=int, default=0,
                     help="also run this many trajectories after one warm-up trajectory (inside an NVTX range "
                          "'trajectories' with --nvtx) and report their device time")
@@ -96,6 +99,28 @@ def main(argv=None) -> int:
             out[f"{k}_ms"] = c.time_kernel(k, a.reps)
             if a.nvtx:
                 torch.cuda.nvtx.range_pop()
+    if a.dd:
+        import time
+
+        from mag_b200.dd import DomainChmc
+
+        reps = max(2, a.reps)
+        with M.Chmc(tuple(a.dims), **kw) as c:
+            c.hot_start(1)
+            c.trajectory()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                c.trajectory()
+            t_one = (time.perf_counter() - t0) / reps
+        with DomainChmc(tuple(a.dims), a.dd, 2, **kw) as d:
+            d.hot_start(1)
+            d.trajectory()
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                d.trajectory()
+            t_dd = (time.perf_counter() - t0) / reps
+        out["dd"] = {"nshards": a.dd, "halo": 2, "undivided_eager_traj_ms": t_one * 1e3,
+                     "split_traj_ms": t_dd * 1e3, "ratio": t_dd / t_one}
     if a.probe:
         from mag_b200.field_hmc import probe_fma_peak
 

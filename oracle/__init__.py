@@ -104,6 +104,10 @@ def lib():
             "mo_gauge_transform": (None, [ip, dp, dp]),
             "mo_demon_sweeps": (None, [ip, dp, ctypes.c_uint64, ctypes.c_int, ctypes.c_double, dp,
                                        ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), dp]),
+            "mo_multi_forces": (None, [pp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp]),
+            "mo_multi_hamiltonian": (None, [pp, ctypes.c_double, ctypes.c_double, dp, dp, dp, dp, dp]),
+            "mo_multi_trajectory": (None, [pp, ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp,
+                                           ctypes.c_double, dp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -321,4 +325,38 @@ def demon_sweeps(dims, U, seed: int, n_sweeps: int, e_max: float):
     lib().mo_demon_sweeps(_dims(dims), _dp(U), int(seed), int(n_sweeps), float(e_max), _dp(E), ctypes.byref(a),
                           ctypes.byref(r), _dp(dev))
     return U, E, a.value, r.value, dev
+
+
+# ------------------------------------------------------------ two-level coupling
+def coarse_dims(dims):
+    return tuple(int(d) // 2 for d in dims)
+
+
+def multi_forces(p: Params, rho: float, eta_sqr: float, Uf, Uc):
+    """field-multi.h get_Fforce / get_Cforce: (fine force, coarse force)."""
+    Ff, Fc = np.zeros_like(Uf), np.zeros_like(Uc)
+    lib().mo_multi_forces(ctypes.byref(p), rho, eta_sqr, _dp(_m4(Uf)), _dp(_m4(Uc)), _dp(Ff), _dp(Fc))
+    return Ff, Fc
+
+
+def multi_hamiltonian(p: Params, rho: float, eta_sqr: float, Uf, Pf, Uc, Pc):
+    """field-multi.h get_hamiltonian_multi: {H, kinetic, fine action, coupling}."""
+    out = (ctypes.c_double * 4)()
+    lib().mo_multi_hamiltonian(ctypes.byref(p), rho, eta_sqr, _dp(_m4(Uf)), _dp(_m4(Pf)), _dp(_m4(Uc)),
+                               _dp(_m4(Pc)), out)
+    return {"H": out[0], "kinetic": out[1], "fine": out[2], "eta": out[3]}
+
+
+def multi_trajectory(p: Params, rho: float, eta_sqr: float, traj_index: int, Uf, Pf, Uc, Pc, uniform: float):
+    """One run_hmc_multi trajectory with given momenta and uniform: (Uf, Uc, record)."""
+    Uf, Uc = _m4(Uf).copy(), _m4(Uc).copy()
+    out = (ctypes.c_double * 6)()
+    lib().mo_multi_trajectory(ctypes.byref(p), rho, eta_sqr, int(traj_index), _dp(Uf), _dp(_m4(Pf)), _dp(Uc),
+                              _dp(_m4(Pc)), uniform, out)
+    return Uf, Uc, {"h_old": out[0], "h_new": out[1], "delta_h": out[2], "accept": int(out[3]),
+                    "reunit_fine": out[4], "reunit_coarse": out[5]}
+
+
+def _m4(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
 

@@ -1204,3 +1204,354 @@ void mo_demon_sweeps(const int dims[4], double* U, uint64_t seed, int n_sweeps, 
 }
 
 }  // extern "C"
+
+// ================================================================ two-level coupling
+// A fine field U_f (the lattice) and a coarse field U_c (every extent halved)
+// coupled through the stout-smeared blocked links of the fine field
+// (field-multi.h:22-45, 309-656, 659-683, 685-756, 758-900):
+//   H = K_f + K_c + S_f(U_f) - 1/eta^2 sum_{coarse x, mu} ReTr(U_c(x,mu)^dag e^{iQ(2x,mu)} V(2x,mu)),
+//   V(y,mu) = U_f(y,mu) U_f(y+mu,mu)          (get_U),
+//   Q(y,mu) = -i rho TA(stp(y,mu) V(y,mu)^dag) (get_Q, stp = get_staple_rect, field-hmc.h:244-258).
+// The reference reads rho and eta_sqr from globals that are not in its tree;
+// here they are arguments.  Both fields are unconstrained (mag = 0).
+namespace {
+
+M3 multi_V(const Field& f, const int x[4], int mu) {  // field-multi.h:24-27 get_U
+    int y[4] = {x[0], x[1], x[2], x[3]};
+    y[mu]++;
+    return f.at(x, mu) * f.at(y, mu);
+}
+
+M3 staple_rect(const Field& f, const int x[4], int mu) {  // field-hmc.h:244-258 get_staple_rect
+    M3 s = zero3();
+    for (int nu = 0; nu < 4; nu++) {
+        if (nu == mu) continue;
+        const int d1[4] = {nu, mu, mu, nu + 4};
+        s += path_product(f, x, d1, 4);
+        const int d2[4] = {nu + 4, mu, mu, nu};
+        s += path_product(f, x, d2, 4);
+    }
+    return s;
+}
+
+M3 multi_Q(const Field& f, const int x[4], int mu, double rho) {  // field-multi.h:29-35 get_Q
+    const M3 Omega = ta(staple_rect(f, x, mu) * dag(multi_V(f, x, mu)));
+    return cscale(Omega, cplx(0.0, -rho));
+}
+
+// field-matrix.h:177-197 get_path_ordered_product_insertion (-1 marks the insertion)
+M3 path_insertion(const Field& f, const int x[4], const int dir[6], const M3& ins) {
+    M3 m = unit3();
+    int y[4] = {x[0], x[1], x[2], x[3]};
+    for (int i = 0; i < 6; i++) {
+        const int d = dir[i];
+        if (d == -1) {
+            m = m * ins;
+        } else if (d < 4) {
+            m = m * f.at(y, d);
+            y[d]++;
+        } else {
+            y[d - 4]--;
+            m = m * dag(f.at(y, d - 4));
+        }
+    }
+    return m;
+}
+
+// field-multi.h:378-407 stout_type: {type, direction}
+void stout_type(const int x[4], int mu, int out[2]) {
+    int cnt[4], n = 0;
+    for (int i = 0; i < 4; i++)
+        if (x[i] % 2 == 1) cnt[n++] = i;
+    out[0] = 0; out[1] = 0;
+    if (n == 0) { out[0] = 1; }
+    else if (n == 1) {
+        if (cnt[0] == mu) out[0] = 3;
+        else { out[0] = 2; out[1] = cnt[0]; }
+    } else if (n == 2) {
+        if (cnt[0] == mu) { out[0] = 4; out[1] = cnt[1]; }
+        else if (cnt[1] == mu) { out[0] = 4; out[1] = cnt[0]; }
+    }
+}
+
+inline void halve(const int y[4], int c[4]) {
+    for (int i = 0; i < 4; i++) c[i] = y[i] / 2;  // y even (possibly negative): exact
+}
+
+// field-multi.h:309-340 get_eta_energy
+DD eta_energy(const Lat& lc, const Field& ff, const Field& fc, double rho, double eta_sqr) {
+    std::vector<double> e(lc.V);
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lc.V; s++) {
+        int x[4];
+        lc.coord(s, x);
+        const int y[4] = {2 * x[0], 2 * x[1], 2 * x[2], 2 * x[3]};
+        double acc = 0.0;
+        for (int mu = 0; mu < 4; mu++) {
+            const M3 Gb = expiQ(multi_Q(ff, y, mu, rho)) * multi_V(ff, y, mu);
+            acc += retr(dag(fc.at(s, mu)) * Gb) / eta_sqr;
+        }
+        e[s] = acc;
+    }
+    return dd_neg(dd_sum(e));
+}
+
+// field-multi.h:659-683 get_Cforce
+void coarse_force(const Lat& lc, const Field& ff, const Field& fc, double* Fc, double rho, double eta_sqr) {
+    Field fo{&lc, Fc};
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lc.V; s++) {
+        int x[4];
+        lc.coord(s, x);
+        const int y[4] = {2 * x[0], 2 * x[1], 2 * x[2], 2 * x[3]};
+        for (int mu = 0; mu < 4; mu++) {
+            const M3 G = expiQ(multi_Q(ff, y, mu, rho)) * multi_V(ff, y, mu);
+            fo.at(s, mu) = cscale(ta(fc.at(s, mu) * dag(G)), cplx(0.0, 1.0 / eta_sqr));
+        }
+    }
+}
+
+// field-multi.h:409-656 get_Fforce: the thin gauge force of the fine field plus the
+// derivative of the coupling through V and through the blocked staples, the
+// insertion paths of the reference listed per stout_type
+void fine_force(const mo_params* p, const Lat& lf, const Lat& lc, const Field& ff, const Field& fc, double* Ff,
+                double rho, double eta_sqr) {
+    Field fo{&lf, Ff};
+    const cplx ib3(0.0, p->beta / 3.0);
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lf.V; s++) {
+        int x[4];
+        lf.coord(s, x);
+        for (int mu = 0; mu < 4; mu++) {
+            const M3 st = p->action == 1 ? action_staple_dagger(ff, x, mu, p) : staple_dagger(ff, x, mu);
+            fo.at(s, mu) = cscale(ta(ff.at(s, mu) * st), ib3);
+        }
+    }
+    // Lambda of every coarse link (field-multi.h:459-469)
+    std::vector<double> Cl(lc.V * 72);
+    Field fl{&lc, Cl.data()};
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lc.V; s++) {
+        int x[4];
+        lc.coord(s, x);
+        const int y[4] = {2 * x[0], 2 * x[1], 2 * x[2], 2 * x[3]};
+        for (int mu = 0; mu < 4; mu++)
+            fl.at(s, mu) = compute_lambda(multi_Q(ff, y, mu, rho), dag(fc.at(s, mu)), multi_V(ff, y, mu));
+    }
+    const cplx ir(0.0, rho);
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lf.V; s++) {
+        int x[4];
+        lf.coord(s, x);
+        for (int mu = 0; mu < 4; mu++) {
+            M3 t = zero3();
+            int sx[4] = {x[0], x[1], x[2], x[3]};
+            sx[mu]++;  // every insertion path starts at x + mu
+            int tn[2];
+            stout_type(x, mu, tn);
+            int y[4], c[4];
+            auto set_y = [&](int d1, int k1, int d2, int k2) {
+                for (int i = 0; i < 4; i++) y[i] = x[i];
+                if (d1 >= 0) y[d1] += k1;
+                if (d2 >= 0) y[d2] += k2;
+                halve(y, c);
+            };
+            switch (tn[0]) {
+                case 1: {
+                    int z[4] = {x[0], x[1], x[2], x[3]};
+                    z[mu]++;
+                    set_y(-1, 0, -1, 0);
+                    t += ff.at(z, mu) * dag(fc.at(c, mu)) * expiQ(multi_Q(ff, x, mu, rho));
+                    for (int nu = 0; nu < 4; nu++) {
+                        if (nu == mu) continue;
+                        set_y(-1, 0, -1, 0);
+                        { const int d[6] = {mu, nu, mu + 4, mu + 4, nu + 4, -1};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), ir); }
+                        { const int d[6] = {mu, nu + 4, mu + 4, mu + 4, nu, -1};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), ir); }
+                        { const int d[6] = {nu, nu, mu + 4, nu + 4, nu + 4, -1};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, nu)), -ir); }
+                        set_y(nu, -2, -1, 0);
+                        { const int d[6] = {nu + 4, nu + 4, mu + 4, -1, nu, nu};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, nu)), ir); }
+                    }
+                    break;
+                }
+                case 2: {
+                    const int o = tn[1];
+                    set_y(o, -1, -1, 0);
+                    { const int d[6] = {mu, o + 4, mu + 4, mu + 4, -1, o};
+                      t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), -ir); }
+                    set_y(o, 1, -1, 0);
+                    { const int d[6] = {mu, o, mu + 4, mu + 4, -1, o + 4};
+                      t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), -ir); }
+                    break;
+                }
+                case 3: {
+                    set_y(mu, -1, -1, 0);
+                    t += dag(fc.at(c, mu)) * expiQ(multi_Q(ff, y, mu, rho)) * ff.at(y, mu);
+                    for (int nu = 0; nu < 4; nu++) {
+                        if (nu == mu) continue;
+                        set_y(mu, -1, -1, 0);
+                        { const int d[6] = {nu, mu + 4, mu + 4, nu + 4, -1, mu};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), ir); }
+                        { const int d[6] = {nu + 4, mu + 4, mu + 4, nu, -1, mu};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), ir); }
+                        set_y(mu, 1, -1, 0);
+                        { const int d[6] = {-1, nu, nu, mu + 4, nu + 4, nu + 4};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, nu)), ir); }
+                        set_y(mu, 1, nu, -2);
+                        { const int d[6] = {nu + 4, nu + 4, -1, mu + 4, nu, nu};
+                          t += cscale(path_insertion(ff, sx, d, fl.at(c, nu)), -ir); }
+                    }
+                    break;
+                }
+                case 4: {
+                    const int o = tn[1];
+                    set_y(o, -1, mu, -1);
+                    { const int d[6] = {o + 4, mu + 4, mu + 4, -1, o, mu};
+                      t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), -ir); }
+                    set_y(o, 1, mu, -1);
+                    { const int d[6] = {o, mu + 4, mu + 4, -1, o + 4, mu};
+                      t += cscale(path_insertion(ff, sx, d, fl.at(c, mu)), -ir); }
+                    break;
+                }
+                default: break;
+            }
+            fo.at(s, mu) += cscale(ta(ff.at(s, mu) * t), cplx(0.0, 1.0 / eta_sqr));
+        }
+    }
+}
+
+// K = sum ReTr(P^2) / 2 over every link (field-multi.h:270-296 get_kinetic_energy, m = 1)
+DD kinetic_all(const Lat& lat, const double* P) {
+    std::vector<double> ks(lat.V);
+    const Field fp{&lat, const_cast<double*>(P)};
+#pragma omp parallel for schedule(static)
+    for (long s = 0; s < lat.V; s++) {
+        double acc = 0.0;
+        for (int mu = 0; mu < 4; mu++) acc += retr(fp.at(s, mu) * fp.at(s, mu));
+        ks[s] = acc;
+    }
+    return dd_mul(dd_sum(ks), 0.5);
+}
+
+struct MultiH {
+    DD kin, fine, eta;
+};
+// field-multi.h:342-376 get_hamiltonian_multi
+MultiH multi_hamiltonian(const mo_params* p, const Lat& lf, const Lat& lc, const double* Uf, const double* Pf,
+                         const double* Uc, const double* Pc, double rho, double eta_sqr) {
+    mo_params thin = *p;
+    thin.n_stout = 0;
+    DD a[3];
+    action(&thin, lf, Uf, a);
+    const Field ff{&lf, const_cast<double*>(Uf)}, fc{&lc, const_cast<double*>(Uc)};
+    return MultiH{dd_add(kinetic_all(lf, Pf), kinetic_all(lc, Pc)), a[2], eta_energy(lc, ff, fc, rho, eta_sqr)};
+}
+
+// field-multi.h:685-756 force_gradient_integrator_multi
+void multi_integrate(const mo_params* p, const Lat& lf, const Lat& lc, double* Uf, double* Pf, double* Uc, double* Pc,
+                     double rho, double eta_sqr, double maxdev[2]) {
+    mo_params q = *p;
+    q.mag = 0;
+    const size_t nf = (size_t)lf.V * 72, nc = (size_t)lc.V * 72;
+    std::vector<double> Ff(nf), Fc(nc), Ufa(nf), Uca(nc);
+    const double dt = p->tau / p->n_steps;
+    const double alpha = (3. - std::sqrt(3.)) * dt / 6.;
+    const double beta = dt / std::sqrt(3.);
+    const double gamma = (2. - std::sqrt(3.)) * dt * dt / 12.;
+    mo_params qc = q;
+    for (int i = 0; i < 4; i++) qc.dims[i] = lc.L[i];
+    auto forces = [&](double* uf, double* uc) {
+        const Field ff{&lf, uf}, fc{&lc, uc};
+        fine_force(p, lf, lc, ff, fc, Ff.data(), rho, eta_sqr);
+        coarse_force(lc, ff, fc, Fc.data(), rho, eta_sqr);
+    };
+    auto drift = [&](double eps) {
+        evolve_gauge(&q, lf, Uf, Pf, eps);
+        evolve_gauge(&qc, lc, Uc, Pc, eps);
+    };
+    auto fg_kick = [&]() {
+        forces(Uf, Uc);
+        std::memcpy(Ufa.data(), Uf, nf * sizeof(double));
+        std::memcpy(Uca.data(), Uc, nc * sizeof(double));
+        evolve_gauge(&q, lf, Ufa.data(), Ff.data(), gamma);
+        evolve_gauge(&qc, lc, Uca.data(), Fc.data(), gamma);
+        forces(Ufa.data(), Uca.data());
+        evolve_momentum(lf, Pf, Ff.data(), 0.5 * dt, 1.0);
+        evolve_momentum(lc, Pc, Fc.data(), 0.5 * dt, 1.0);
+    };
+    drift(alpha);
+    for (int i = 0; i < p->n_steps; i++) {
+        fg_kick();
+        drift(beta);
+        fg_kick();
+        drift(i < p->n_steps - 1 ? 2. * alpha : alpha);
+    }
+    maxdev[0] = reunitarize(lf, Uf);
+    maxdev[1] = reunitarize(lc, Uc);
+}
+
+void coarse_dims(const int d[4], int c[4]) {
+    for (int i = 0; i < 4; i++) c[i] = d[i] / 2;
+}
+
+}  // namespace
+
+extern "C" {
+
+// fine force Ff (fine lattice) and coarse force Fc (every extent halved)
+void mo_multi_forces(const mo_params* p, double rho, double eta_sqr, const double* Uf, const double* Uc, double* Ff,
+                     double* Fc) {
+    int cd[4];
+    coarse_dims(p->dims, cd);
+    Lat lf(p->dims), lc(cd);
+    const Field ff{&lf, const_cast<double*>(Uf)}, fc{&lc, const_cast<double*>(Uc)};
+    fine_force(p, lf, lc, ff, fc, Ff, rho, eta_sqr);
+    coarse_force(lc, ff, fc, Fc, rho, eta_sqr);
+}
+
+// out = {H, kinetic (both levels), fine gauge action, coupling energy}
+void mo_multi_hamiltonian(const mo_params* p, double rho, double eta_sqr, const double* Uf, const double* Pf,
+                          const double* Uc, const double* Pc, double out[4]) {
+    int cd[4];
+    coarse_dims(p->dims, cd);
+    Lat lf(p->dims), lc(cd);
+    const MultiH h = multi_hamiltonian(p, lf, lc, Uf, Pf, Uc, Pc, rho, eta_sqr);
+    out[0] = dd_val(dd_add(dd_add(h.kin, h.fine), h.eta));
+    out[1] = dd_val(h.kin);
+    out[2] = dd_val(h.fine);
+    out[3] = dd_val(h.eta);
+}
+
+// one trajectory of run_hmc_multi (field-multi.h:858-900) with given momenta and uniform;
+// out = {H_old, H_new, Delta H, accept, reunit fine, reunit coarse}
+void mo_multi_trajectory(const mo_params* p, double rho, double eta_sqr, int traj_index, double* Uf,
+                         const double* Pf, double* Uc, const double* Pc, double uniform, double out[6]) {
+    int cd[4];
+    coarse_dims(p->dims, cd);
+    Lat lf(p->dims), lc(cd);
+    const size_t nf = (size_t)lf.V * 72, nc = (size_t)lc.V * 72;
+    std::vector<double> pf(Pf, Pf + nf), pc(Pc, Pc + nc), uf0(Uf, Uf + nf), uc0(Uc, Uc + nc);
+    const MultiH a = multi_hamiltonian(p, lf, lc, Uf, pf.data(), Uc, pc.data(), rho, eta_sqr);
+    double dev[2];
+    multi_integrate(p, lf, lc, Uf, pf.data(), Uc, pc.data(), rho, eta_sqr, dev);
+    const MultiH b = multi_hamiltonian(p, lf, lc, Uf, pf.data(), Uc, pc.data(), rho, eta_sqr);
+    const double dh = dd_val(dd_add(dd_add(dd_add(b.kin, dd_neg(a.kin)), dd_add(b.fine, dd_neg(a.fine))),
+                                    dd_add(b.eta, dd_neg(a.eta))));
+    bool acc = uniform < std::exp(-dh);
+    if (traj_index < p->n_forced) acc = true;
+    if (!acc) {
+        std::memcpy(Uf, uf0.data(), nf * sizeof(double));
+        std::memcpy(Uc, uc0.data(), nc * sizeof(double));
+    }
+    out[0] = dd_val(dd_add(dd_add(a.kin, a.fine), a.eta));
+    out[1] = dd_val(dd_add(dd_add(b.kin, b.fine), b.eta));
+    out[2] = dh;
+    out[3] = acc ? 1.0 : 0.0;
+    out[4] = dev[0];
+    out[5] = dev[1];
+}
+
+}  // extern "C"

@@ -91,6 +91,14 @@ void mo_gauge_transform(const int dims[4], double* U, const double* G);
 void mo_demon_sweeps(const int dims[4], double* U, uint64_t seed, int n_sweeps, double e_max, double* E_trace,
                      int64_t* accept, int64_t* reject, double* reunit);
 
+/* two-level coupling (field-multi.h): coarse dims = dims / 2; rho, eta_sqr as parameters */
+void mo_multi_forces(const mo_params* p, double rho, double eta_sqr, const double* Uf, const double* Uc, double* Ff,
+                     double* Fc);
+void mo_multi_hamiltonian(const mo_params* p, double rho, double eta_sqr, const double* Uf, const double* Pf,
+                          const double* Uc, const double* Pc, double out[4]);
+void mo_multi_trajectory(const mo_params* p, double rho, double eta_sqr, int traj_index, double* Uf,
+                         const double* Pf, double* Uc, const double* Pc, double uniform, double out[6]);
+
 #ifdef __cplusplus
 }
 #endif

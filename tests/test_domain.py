@@ -109,3 +109,78 @@ def test_split_device_rng_repeats_the_undivided_run():
             rd = d.trajectory(refresh_momenta=True)
             assert rd["accept"] == r1["accept"] and abs(rd["delta_h"] - r1["delta_h"]) < 1e-10
         assert np.abs(d.get_gauge() - c.get_gauge()).max() < 1e-13
+
+
+def _shard_proc(rank, world, port, q, halo):
+    import datetime
+    import os
+
+    import torch
+    import torch.distributed as dist
+
+    import oracle as O
+    from mag_b200.halo import ShardChmc, TorchHaloExchange, interior_of, slab_of
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        torch.cuda.set_device(0)
+        U = O.gen_hot(DIMS, 12)
+        P = O.gen_momenta(DIMS, 5, 0)
+        ex = TorchHaloExchange()
+        with ShardChmc(DIMS, world, rank, halo, exchange=ex, **KW) as c:
+            c.set_gauge(slab_of(U, DIMS, world, rank, halo))
+            F = interior_of(c.get_force(), DIMS, world, halo)
+            c.init_momentum(slab_of(P, DIMS, world, rank, halo))
+            c.set_uniforms([O.gen_uniform(5, 0)])
+            (r,) = c.trajectory(refresh_momenta=False)
+            Ui = interior_of(c.get_gauge(), DIMS, world, halo)
+        q.put((rank, F, r["delta_h"], r["accept"], r["h_old"], Ui))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_one_slab_per_process_through_the_halo_callback():
+    """mag_shard_create + mag_set_halo_fn with mag_b200.halo.TorchHaloExchange: two processes on
+    the one GPU, each holding one slab, exchanging halos and sums through gloo (host copies; no
+    kernel waits on another process).  Force, Delta H, accept bit and links equal the undivided
+    lattice's."""
+    import socket
+
+    import torch.multiprocessing as mp
+
+    import oracle as O
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    world, halo = 2, 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shard_proc, args=(r, world, port, q, halo)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=300) for _ in range(world)], key=lambda x: x[0])
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    U = O.gen_hot(DIMS, 12)
+    P = O.gen_momenta(DIMS, 5, 0)
+    with M.Chmc(DIMS, **KW) as c:
+        c.set_gauge(U)
+        F1 = c.get_force()
+        c.init_momentum(P)
+        c.set_uniforms([O.gen_uniform(5, 0)])
+        (r1,) = c.trajectory(refresh_momenta=False)
+        U1 = c.get_gauge()
+    F = np.concatenate([r[1] for r in res])
+    assert np.abs(F - F1).max() <= 1e-14 * np.abs(F1).max()
+    for r in res:
+        assert r[3] == r1["accept"]
+        assert abs(r[2] - r1["delta_h"]) < 1e-10
+        assert abs(r[4] - r1["h_old"]) <= 1e-13 * abs(r1["h_old"])
+    assert np.abs(np.concatenate([r[5] for r in res]) - U1).max() < 1e-13

@@ -306,3 +306,53 @@ def test_demon_sweep_conserves_plaquette_and_rectangle_energy():
     # the demons never leave the window; with a zero window nothing is accepted
     _, E0, acc0, rej0, _ = O.demon_sweeps(dims, U, seed=7, n_sweeps=1, e_max=0.0)
     assert acc0 == 0 and np.all(E0 == 0.0)
+
+
+# ------------------------------------------------------------ two-level coupling (field-multi.h)
+MDIMS = (4, 4, 4, 8)
+
+
+def _multi_S(p, rho, eta2, Uf, Uc):
+    Zf, Zc = np.zeros_like(Uf), np.zeros_like(Uc)
+    return O.multi_hamiltonian(p, rho, eta2, Uf, Zf, Uc, Zc)["H"]
+
+
+@pytest.mark.parametrize("action", [0, 1])
+def test_multi_forces_are_minus_the_coupled_action_derivative(action):
+    """get_Fforce / get_Cforce restated (the reference's insertion paths per stout_type, rho and
+    eta_sqr as parameters) against a central difference of S_gauge(U) + S_eta(U, C): fine links of
+    every stout type (1: all coordinates even, 2: one odd other than mu, 3: mu odd, 4: mu and one
+    other odd, 0: not coupled) and coarse links."""
+    rng = np.random.default_rng(3)
+    Uf, Uc = O.gen_hot(MDIMS, 3), O.gen_hot(O.coarse_dims(MDIMS), 4)
+    p = O.make_params(MDIMS, mag=0, action=action, beta=2.25, c1=-0.331)
+    rho, eta2 = 0.1, 0.5
+    Ff, Fc = O.multi_forces(p, rho, eta2, Uf, Uc)
+    h = 1e-5
+    # (site, mu): (0,0) type 1, (1,0) type 3, (1,1) type 2, (17,2) type 4, (5,3) type 0, (42,0) type 1
+    for field, F, cases in (("fine", Ff, [(0, 0), (1, 0), (1, 1), (17, 2), (5, 3), (42, 0), (85, 3)]),
+                            ("coarse", Fc, [(0, 0), (3, 2), (7, 3)])):
+        for site, mu in cases:
+            X = rand_herm(rng)
+
+            def S(e):
+                a, b = Uf.copy(), Uc.copy()
+                V = a if field == "fine" else b
+                V[site, mu] = O.expiQ(X * e) @ V[site, mu]
+                return _multi_S(p, rho, eta2, a, b)
+
+            fd = (S(h) - S(-h)) / (2 * h)
+            an = -np.trace(X @ F[site, mu]).real
+            assert abs(fd - an) < 2e-7 * max(1.0, abs(an)), (field, site, mu, fd, an)
+
+
+def test_multi_integrator_is_fourth_order():
+    """force_gradient_integrator_multi: |Delta H| falls as dt^4 (16x for half the step)."""
+    Uf, Uc = O.gen_hot(MDIMS, 5), O.gen_hot(O.coarse_dims(MDIMS), 6)
+    Pf, Pc = O.gen_momenta(MDIMS, 7, 0), O.gen_momenta(O.coarse_dims(MDIMS), 8, 0)
+    dh = []
+    for n in (4, 8):
+        p = O.make_params(MDIMS, mag=0, action=1, beta=2.25, c1=-0.331, tau=0.5, n_steps=n)
+        _, _, r = O.multi_trajectory(p, 0.1, 0.5, 0, Uf, Pf, Uc, Pc, 0.0)
+        dh.append(abs(r["delta_h"]))
+    assert 10.0 < dh[0] / dh[1] < 25.0, dh
