@@ -314,12 +314,15 @@ struct mag_ctx {
         for (int c = 0; c < n; c++)
             for (long k = hc[c].off / MAG_CHUNK; k < (hc[c].off + hc[c].V + MAG_CHUNK - 1) / MAG_CHUNK; k++)
                 c2c[k] = (uint16_t)c;
-        MAG_CUDA(cudaMemcpy(d_chains, hc.data(), sizeof(ChainInfo) * n, cudaMemcpyHostToDevice));
-        MAG_CUDA(cudaMemcpy(d_c2c, c2c.data(), sizeof(uint16_t) * nchunk, cudaMemcpyHostToDevice));
+        // on the context's stream (a pageable cudaMemcpy may return before its DMA lands, and the
+        // non-blocking stream would not wait for it); the sync at the end of init covers them
+        MAG_CUDA(cudaMemcpyAsync(d_chains, hc.data(), sizeof(ChainInfo) * n, cudaMemcpyHostToDevice, stream));
+        MAG_CUDA(cudaMemcpyAsync(d_c2c, c2c.data(), sizeof(uint16_t) * nchunk, cudaMemcpyHostToDevice, stream));
         MAG_TRY(alloc((void**)&d_stream_index, sizeof(unsigned long long) * n));
         std::vector<unsigned long long> sidx(n);
         for (int c = 0; c < n; c++) sidx[c] = (unsigned long long)c;
-        MAG_CUDA(cudaMemcpy(d_stream_index, sidx.data(), sizeof(unsigned long long) * n, cudaMemcpyHostToDevice));
+        MAG_CUDA(cudaMemcpyAsync(d_stream_index, sidx.data(), sizeof(unsigned long long) * n,
+                                 cudaMemcpyHostToDevice, stream));
         h_stream_index = sidx;
         geom = DevGeom{d_chains, d_c2c, vpad, n, d_stream_index, 0, 0, 0};
 
@@ -1106,7 +1109,9 @@ int demon_sweeps(mag_ctx* ctx, const std::vector<int>& chains, const std::vector
         MAG_TRY(ctx->alloc((void**)&ctx->d_demon_tables, sizeof(DemonTables)));
         MAG_TRY(ctx->alloc((void**)&ctx->d_demon, sizeof(DemonState) * ctx->nchain));
         MAG_TRY(ctx->alloc((void**)&ctx->d_demon_jobs, sizeof(DemonJob) * ctx->nchain));
-        MAG_CUDA(cudaMemcpy(ctx->d_demon_tables, tabs.get(), sizeof(DemonTables), cudaMemcpyHostToDevice));
+        MAG_CUDA(cudaMemcpyAsync(ctx->d_demon_tables, tabs.get(), sizeof(DemonTables), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        MAG_TRY(ctx->sync("demon tables"));
     }
     // one chain: its AoS copy in the staging buffer; several: the ensemble-wide AoS buffer
     double* aos = ctx->staging;
@@ -1687,7 +1692,8 @@ int ensure_crc_tab(mag_ctx* ctx, size_t seg) {
     if (ctx->crc_tab_seg == seg) return MAG_OK;
     uint32_t tab[4][256];
     nersc::crc32_shift_tables(seg, tab);
-    MAG_CUDA(cudaMemcpy(ctx->d_crc_tab, tab, sizeof(tab), cudaMemcpyHostToDevice));
+    MAG_CUDA(cudaMemcpyAsync(ctx->d_crc_tab, tab, sizeof(tab), cudaMemcpyHostToDevice, ctx->stream));
+    MAG_TRY(ctx->sync("crc tables"));
     ctx->crc_tab_seg = seg;
     return MAG_OK;
 }
@@ -1966,8 +1972,14 @@ struct DdHook : HaloHook {
         if (reunit)
             for (int r = 0; r < d->n; r++) rmax = std::max(rmax, d->host_reunit[r]);  // non-negative doubles
         d->barrier();
-        if (e == cudaSuccess) e = cudaMemcpy(c->sums, tot.data(), sizeof(dd2) * NUM_SLOTS, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && reunit) e = cudaMemcpy(c->reunit, &rmax, sizeof(rmax), cudaMemcpyHostToDevice);
+        // on the shard's stream (a plain cudaMemcpy from pageable memory may return before the
+        // copy lands, and the shard's non-blocking stream would not wait for it), then synchronised
+        // because the host values live in this frame
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(c->sums, tot.data(), sizeof(dd2) * NUM_SLOTS, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && reunit)
+            e = cudaMemcpyAsync(c->reunit, &rmax, sizeof(rmax), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
         if (e != cudaSuccess) return fail(MAG_ERR_CUDA, std::string("halo reduce: ") + cudaGetErrorString(e));
         return MAG_OK;
     }
@@ -2057,9 +2069,9 @@ struct CallbackHook : HaloHook {
             h[slots[k]] = dd2{sum, lo - (sum - hi)};
         }
         std::memcpy(&r, &rmax, sizeof(r));
-        MAG_CUDA(cudaMemcpy(c->sums, h.data(), sizeof(dd2) * NUM_SLOTS, cudaMemcpyHostToDevice));
-        if (reunit) MAG_CUDA(cudaMemcpy(c->reunit, &r, sizeof(r), cudaMemcpyHostToDevice));
-        return MAG_OK;
+        MAG_CUDA(cudaMemcpyAsync(c->sums, h.data(), sizeof(dd2) * NUM_SLOTS, cudaMemcpyHostToDevice, c->stream));
+        if (reunit) MAG_CUDA(cudaMemcpyAsync(c->reunit, &r, sizeof(r), cudaMemcpyHostToDevice, c->stream));
+        return c->sync("halo reduce");
     }
 };
 
