@@ -5,6 +5,11 @@
   against the oracle's records in tests/golden/run_16x16x16x32_3stout.json: H_old to 1e-12
   relative, Delta H to 1e-9 absolute, the same accept bit and the plaquette to 1e-12 on every
   trajectory.
+* The 32^4 lattice of the mixed-versus-FP64 comparison (same action and smearing, sixteen
+  force-gradient steps) for two trajectories against tests/golden/run_32x32x32x32_3stout.json,
+  in FP64 at those bars and in mixed precision at the mixed ones (below).
+* The 48^3 x 96 lattice of the Wilson-loop workload: Wilson loops, plaquettes and action sums
+  of a hot start against tests/golden/hot_48x48x48x96_wloops.json.
 * The mixed-precision path (FP32 staples, force and smearing on FP32 copies of the FP64
   master links; FP64 link integration, reunitarisation and Hamiltonian) from a thermalised
   6^4 configuration with three stout levels, against the oracle on the same momenta and
@@ -48,26 +53,82 @@ def _gpu_trajectory(c, U, P, u, chain_count=1):
     return r
 
 
-def test_config2_twenty_trajectories_against_the_oracle_records():
-    with open(os.path.join(GOLDEN, "run_16x16x16x32_3stout.json")) as f:
+def _replay_records(name, precision):
+    """Replays a fixture's run (same start, momenta and uniforms) on the GPU; returns
+    (GPU records, oracle records)."""
+    with open(os.path.join(GOLDEN, name)) as f:
         fx = json.load(f)
     dims = tuple(fx["dims"])
     p = fx["params"]
     seed = fx["rng_seed"]
+    out = []
     with M.Chmc(dims, mag=p["mag"], action="iwasaki", beta=p["beta"], c1=p["c1"], rho=p["rho"],
-                n_stout=p["n_stout"], tau=p["tau"], n_steps=p["n_steps"], precision="fp64", seed=seed) as c:
+                n_stout=p["n_stout"], tau=p["tau"], n_steps=p["n_steps"], precision=precision, seed=seed) as c:
         c.set_gauge(O.gen_hot(dims, fx["hot_seed"]))
-        accepts = []
-        for t, o in enumerate(fx["records"]):
+        for t in range(len(fx["records"])):
             c.init_momentum(O.gen_momenta(dims, seed, t))
             c.set_uniforms([O.gen_uniform(seed, t)])
             (g,) = c.trajectory(refresh_momenta=False)
-            assert abs(g["h_old"] - o["h_old"]) <= 1e-12 * abs(o["h_old"]), t
-            assert abs(g["delta_h"] - o["delta_h"]) < 1e-9, (t, g["delta_h"], o["delta_h"])
-            assert g["accept"] == o["accept"], t
-            assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-12, t
-            accepts.append(g["accept"])
-    assert len(accepts) == 20
+            out.append(g)
+    return out, fx["records"]
+
+
+def _check_fp64_records(recs, ref):
+    for t, (g, o) in enumerate(zip(recs, ref)):
+        assert abs(g["h_old"] - o["h_old"]) <= 1e-12 * abs(o["h_old"]), t
+        assert abs(g["delta_h"] - o["delta_h"]) < 1e-9, (t, g["delta_h"], o["delta_h"])
+        assert g["accept"] == o["accept"], t
+        assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-12, t
+
+
+def test_config2_twenty_trajectories_against_the_oracle_records():
+    recs, ref = _replay_records("run_16x16x16x32_3stout.json", "fp64")
+    assert len(recs) == 20
+    _check_fp64_records(recs, ref)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_32x32x32x32_trajectories_against_the_oracle_records(precision):
+    """The lattice the mixed-versus-FP64 comparison is stated on, at full size: FP64 at the
+    FP64 bars; mixed with the plaquette within 1e-7 of the oracle, the same accept bits and
+    Delta H within 5e-3."""
+    recs, ref = _replay_records("run_32x32x32x32_3stout.json", precision)
+    assert len(recs) == 2
+    if precision == "fp64":
+        _check_fp64_records(recs, ref)
+        return
+    for t, (g, o) in enumerate(zip(recs, ref)):
+        h_tol = 1e-12 if t == 0 else 1e-7
+        assert abs(g["h_old"] - o["h_old"]) <= h_tol * abs(o["h_old"]), t
+        assert abs(g["delta_h"] - o["delta_h"]) < 5e-3, (t, g["delta_h"], o["delta_h"])
+        assert g["accept"] == o["accept"], t
+        assert abs(g["avg_plaquette"] - o["avg_plaquette"]) < 1e-7, t
+
+
+def test_48x48x48x96_measurements_against_the_oracle_records():
+    """The Wilson-loop workload's lattice at full size (48^3 x 96): a device hot start from
+    Philox seed 6 (equal to the oracle's host-generated one to rounding) measured in the
+    workload's context (mixed, three stout levels, beta 2.37; the measurements read the FP64
+    master links) against the oracle: planar and off-axis Wilson loops, the average and the
+    constrained plaquette to 1e-12; the thin plaquette and rectangle sums to 1e-12 relative."""
+    with open(os.path.join(GOLDEN, "hot_48x48x48x96_wloops.json")) as f:
+        fx = json.load(f)
+    dims = tuple(fx["dims"])
+    with M.Chmc(dims, mag=2, action="iwasaki", beta=2.37, c1=-0.331, rho=0.1, n_stout=3, n_steps=16,
+                precision="mixed", seed=1) as c:
+        c.hot_start(fx["hot_seed"])
+        W = c.wilson_loops(8, 8)
+        for e in fx["planar"]:
+            assert abs(W[e["R"] - 1, e["T"] - 1] - e["w"]) < 1e-12, e
+        for e in fx["off_axis"]:
+            assert abs(c.avg_wilson_loop(e["r"], e["T"]) - e["w"]) < 1e-12, e
+        assert abs(c.avg_plaquette() - fx["avg_plaquette"]) < 1e-12
+        assert abs(c.check_constrained_plaquette() - fx["constrained_plaquette_mag2"]) < 1e-12
+    with M.Chmc(dims, mag=2, action="iwasaki", beta=2.37, c1=-0.331, n_stout=0, precision="fp64", seed=1) as c:
+        c.hot_start(fx["hot_seed"])
+        plaq, rect, _ = c.gauge_action()
+    assert abs(plaq - fx["plaq_sum"]) <= 1e-12 * abs(fx["plaq_sum"])
+    assert abs(rect - fx["rect_sum"]) <= 1e-12 * abs(fx["rect_sum"])
 
 
 DIMS6 = (6, 6, 6, 6)
