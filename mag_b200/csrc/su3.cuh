@@ -642,7 +642,8 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
                          // and their derivatives carry powers of q down to q^(n-5)
     const float q = sqrtf(q2);
     const bool qbig = q >= 1.f;
-    // one term: advance Q^{n-1} -> Q^n (and the derivatives), add i^n/n! times it
+    // one term: advance Q^{n-1} -> Q^n (and the derivatives), add i^n/n! times it; the loop
+    // below is unrolled, so n and 1/n are compile-time constants (no division is executed)
     auto term = [&](int n, bool odd) {
         const float na = c0 * d, nb = a + c1 * d, nd = b;
         if (WITH_B) {
@@ -652,8 +653,9 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
             a1 = na1; b1 = nb1; d1 = nd1;
         }
         a = na; b = nb; d = nd;
-        coef /= (float)n;
-        bound *= (qbig || n > 5 ? q : 1.f) / (float)n;
+        const float inv = 1.f / (float)n;
+        coef *= inv;
+        bound *= (qbig || n > 5 ? q : 1.f) * inv;
         // i^n/n!: real for even n (sign (-1)^{n/2}), imaginary for odd n (sign (-1)^{(n-1)/2})
         const float sgn = ((n >> 1) & 1) ? -coef : coef;
         float* F = odd ? Fi : Fr;
@@ -668,7 +670,7 @@ MAG_HD bool ch_series(float c0, float c1, ch_coef_f& r) {
         }
     };
     // terms in pairs (odd, even) so that the real / imaginary choice is known at compile time
-#pragma unroll 1
+#pragma unroll
     for (int n = 1; n < 40; n += 2) {
         term(n, true);
         term(n + 1, false);
@@ -773,7 +775,7 @@ MAG_HD void ch_invariants_f(const mat3<float>& Q, const mat3<float>& QQ, float& 
     for (int i = 0; i < 3; i++)
 #pragma unroll
         for (int k = 0; k < 3; k++) t3 += QQ.e[i][k].re * Q.e[k][i].re - QQ.e[i][k].im * Q.e[k][i].im;
-    c0 = t3 / 3.f;
+    c0 = t3 * (1.f / 3.f);
     c1 = 0.5f * (QQ.e[0][0].re + QQ.e[1][1].re + QQ.e[2][2].re);
 }
 
