@@ -17,9 +17,10 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmag_b200.so")
 SOURCES = ["kernels_force.cu", "kernels_update.cu", "kernels_wloop.cu", "kernels_nersc.cu", "kernels_demon.cu", "kernels_matrix.cu", "kernels_multi.cu", "mag_api.cu",
+           "mag_nersc_api.cu", "mag_dd.cu", "mag_multi_api.cu",
            "noalloc.cu",
            "nersc_host.cpp"]
-HEADERS = ["su3.cuh", "lattice.cuh", "gauge_ops.cuh", "rng.cuh", "kernels.h", "nersc_host.h"]
+HEADERS = ["su3.cuh", "lattice.cuh", "gauge_ops.cuh", "rng.cuh", "kernels.h", "nersc_host.h", "ctx.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
