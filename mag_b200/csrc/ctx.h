@@ -286,6 +286,7 @@ struct mag_ctx {
             }
             if (q.mag == 1) return fail(MAG_ERR_ARG, "mag = 1 freezes every link (field-hmc.h:331); use 0 or >= 2");
             if (q.action != p.action) return fail(MAG_ERR_ARG, "all chains of an ensemble share the action type");
+            set_divisors(ci);
             ci.V = (int)V;
             ci.off = (int)off;
             ci.mag = q.mag;

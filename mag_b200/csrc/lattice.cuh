@@ -35,8 +35,36 @@ struct ChainInfo {
     // An undivided chain has org3 = 0, L3g = L[3], lo3 = 0, hi3 = L[3], Vg = V.
     int org3, L3g, lo3, hi3;
     int Vg;
+    // divisors of the site decode: x_d = s / (L_0 ... L_{d-1}) mod L_d without a
+    // divide instruction (set_divisors)
+    unsigned dm[3];
+    int ds[3];
     double beta, c0, c1, rho;
 };
+
+// Unsigned division by an invariant d >= 2 (Granlund and Montgomery, "Division
+// by invariant integers using multiplication", 1994): with l = ceil(log2 d) and
+// m = floor(2^32 (2^l - d) / d) + 1, which fits 32 bits because 2^l - d < d,
+//   n / d = (t + ((n - t) >> 1)) >> (l - 1),  t = floor(n m / 2^32),
+// exact for every 32-bit n.
+MAG_HD void set_divisor(unsigned d, unsigned& m, int& sh) {
+    int l = 0;
+    while (l < 32 && (1ull << l) < d) l++;
+    m = (unsigned)(((1ull << 32) * ((1ull << l) - d)) / d + 1);
+    sh = l - 1;
+}
+MAG_HD unsigned div_by(unsigned n, unsigned m, int sh) {
+#if defined(__CUDA_ARCH__)
+    const unsigned t = __umulhi(n, m);
+#else
+    const unsigned t = (unsigned)(((unsigned long long)n * m) >> 32);
+#endif
+    return (t + ((n - t) >> 1)) >> sh;
+}
+// the decode divisors of a chain whose extents L[0..2] are set (each >= 2)
+MAG_HD void set_divisors(ChainInfo& ci) {
+    for (int d = 0; d < 3; d++) set_divisor((unsigned)ci.L[d], ci.dm[d], ci.ds[d]);
+}
 
 struct Site {
     int s;       // local site index inside the chain
@@ -47,11 +75,14 @@ struct Site {
 MAG_HD void decode(const ChainInfo& ci, int s, Site& st) {
     st.s = s;
     st.g = ci.off + s;
-    int r = s;
-    st.x[0] = r % ci.L[0]; r /= ci.L[0];
-    st.x[1] = r % ci.L[1]; r /= ci.L[1];
-    st.x[2] = r % ci.L[2]; r /= ci.L[2];
-    st.x[3] = r;
+    unsigned r = (unsigned)s;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        const unsigned q = div_by(r, ci.dm[d], ci.ds[d]);
+        st.x[d] = (int)(r - q * (unsigned)ci.L[d]);
+        r = q;
+    }
+    st.x[3] = (int)r;
 }
 
 // global index offset of moving k steps (|k| <= L) along d from coordinate xd

@@ -191,6 +191,7 @@ extern "C" int mag_action_sums_noalloc(const int dims[4], const double* d_links,
                                             std::to_string(MAG_NOALLOC_MAX_SITES) +
                                             "-site limit of its static scratch; use mag_action");
     }
+    set_divisors(ci);
     ci.V = (int)V;
     ci.L3g = ci.hi3 = ci.L[3];
     ci.Vg = (int)V;
