@@ -2,6 +2,8 @@
 // slabs in one process (mag_dd_*), or one slab per process with the halos
 // moved through a caller's callback (mag_shard_create, mag_set_halo_fn).
 // The context is in ctx.h.
+#include <exception>
+
 #include "ctx.h"
 
 // A lattice split along x3 into n shards (fetch_expanded_chart's halo exchange,
@@ -27,21 +29,30 @@ struct mag_dd {
     std::vector<std::vector<dd2>> host_sums;
     std::vector<unsigned long long> host_reunit;
     std::vector<double> staging;  // one shard's extended AoS field
-    // reusable barrier for the shard threads
+    // reusable barrier for the shard threads; once broken (a shard thread could not be
+    // started) every wait returns false at once, so the threads that did start finish
     std::mutex mu;
     std::condition_variable cv;
     int arrived = 0;
     long generation = 0;
-    void barrier() {
+    bool broken = false;
+    bool barrier() {
         std::unique_lock<std::mutex> lk(mu);
+        if (broken) return false;
         const long gen = generation;
         if (++arrived == n) {
             arrived = 0;
             generation++;
             cv.notify_all();
         } else {
-            cv.wait(lk, [&] { return generation != gen; });
+            cv.wait(lk, [&] { return generation != gen || broken; });
         }
+        return !broken;
+    }
+    void break_barrier() {
+        std::lock_guard<std::mutex> lk(mu);
+        broken = true;
+        cv.notify_all();
     }
     ~mag_dd() {
         for (auto e : ready) cudaEventDestroy(e);
@@ -52,12 +63,26 @@ struct mag_dd {
     int run(const std::function<int(int)>& fn) {
         std::vector<int> rc(n, MAG_OK);
         std::vector<std::thread> th;
-        for (int r = 0; r < n; r++)
-            th.emplace_back([&, r] {
-                cudaSetDevice(device);
-                rc[r] = fn(r);
-            });
+        bool started = true;
+        for (int r = 0; r < n; r++) {
+            try {
+                th.emplace_back([&, r] {
+                    cudaSetDevice(device);
+                    rc[r] = fn(r);
+                });
+            } catch (const std::exception&) {
+                started = false;
+                break_barrier();
+                break;
+            }
+        }
         for (auto& t : th) t.join();
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            broken = false;
+            arrived = 0;
+        }
+        if (!started) return fail(MAG_ERR_STATE, "domain decomposition: a shard thread could not be started");
         for (int r = 0; r < n; r++)
             if (rc[r] != MAG_OK) return rc[r];
         return MAG_OK;
@@ -75,7 +100,7 @@ struct DdHook : HaloHook {
         const ChainInfo& ci = c->hc[0];
         d->base[s] = base;
         cudaError_t e = cudaEventRecord(d->ready[s], c->stream);
-        d->barrier();
+        if (!d->barrier()) return fail(MAG_ERR_STATE, "halo exchange: the shard group is broken");
         const size_t S3 = (size_t)d->slab_sites(), slab = (size_t)d->h * S3 * unit, plane = unit * (size_t)c->vpad;
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, d->ready[lo], 0);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, d->ready[hi], 0);
@@ -91,7 +116,7 @@ struct DdHook : HaloHook {
                                     cudaMemcpyDeviceToDevice, c->stream);
         }
         if (e == cudaSuccess) e = cudaEventRecord(d->copied[s], c->stream);
-        d->barrier();
+        if (!d->barrier()) return fail(MAG_ERR_STATE, "halo exchange: the shard group is broken");
         // the neighbours' copies out of this shard finish before this shard writes the field again
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, d->copied[lo], 0);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, d->copied[hi], 0);
@@ -107,7 +132,7 @@ struct DdHook : HaloHook {
             e = cudaMemcpyAsync(&d->host_reunit[s], c->reunit, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                 c->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        d->barrier();
+        if (!d->barrier()) return fail(MAG_ERR_STATE, "halo reduce: the shard group is broken");
         // every shard adds the shards' sums in the same order, so all hold the same totals
         std::vector<dd2> tot = mine;
         for (int k = 0; k < nslots; k++) {
@@ -118,7 +143,7 @@ struct DdHook : HaloHook {
         unsigned long long rmax = 0;
         if (reunit)
             for (int r = 0; r < d->n; r++) rmax = std::max(rmax, d->host_reunit[r]);  // non-negative doubles
-        d->barrier();
+        if (!d->barrier()) return fail(MAG_ERR_STATE, "halo reduce: the shard group is broken");
         // on the shard's stream (a plain cudaMemcpy from pageable memory may return before the
         // copy lands, and the shard's non-blocking stream would not wait for it), then synchronised
         // because the host values live in this frame
