@@ -52,7 +52,9 @@ int mag_set_kernel_variant(mag_ctx* ctx, const char* family, int precision, cons
 /* number of kernel nodes in the captured trajectory graph (building it if needed) */
 int mag_graph_kernel_count(mag_ctx* ctx, int* kernels);
 /* measured CUDA-core FMA throughput of this device: precision 0 = FP64 FMA,
-   1 = FP32 FMA, 2 = packed FP32 FMA (fma.rn.f32x2); tflops counts 2 flops per FMA */
+   1 = FP32 FMA, 2 = packed FP32 FMA (fma.rn.f32x2), 3 = packed FP32 FMA whose
+   operands are formed every iteration by swapping, negating one half of and
+   broadcasting changing pairs; tflops counts 2 flops per FMA */
 int mag_probe_fma_peak(int precision, double* tflops);
 /* CRC-32 (zlib) of n host bytes computed the way NERSC export/import does on
    the device: seg-byte segment registers (seg a multiple of 16) chained with

@@ -143,7 +143,7 @@ void launch_links_to_aos_t(LinkPlanes<T> U, int chain_off, int V, double* aos, c
 template <typename T>
 void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s);
 // packed FP32 (fma.rn.f32x2): out holds nblocks * 256 float2
-void launch_ffma2_probe(void* out, int nblocks, int iters, cudaStream_t s);
+void launch_ffma2_probe(void* out, int nblocks, int iters, bool selected_operands, cudaStream_t s);
 
 // sums[c][slot] = sum over the chain's links of ReTr U (avg_real_trace, field-matrix.h:391-405, times 12 V)
 void launch_link_trace_sum(const DevGeom& g, LinkPlanes<double> U, dd2* partial, dd2* sums, int slot,

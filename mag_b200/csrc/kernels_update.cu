@@ -457,14 +457,40 @@ __global__ void k_ffma2_probe(float2* out, int iters) {
     out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// packed FP32 probe with operands formed every iteration from changing pairs:
+// i * pair (halves swapped, one negated) and a broadcast half.  Its throughput
+// and instruction count next to k_ffma2_probe's show whether such operands
+// cost instructions of their own (two packed FMAs per chain and iteration).
+__global__ void k_ffma2_sel_probe(float2* out, int iters) {
+    float2 a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        a[k] = make_float2((float)(threadIdx.x + k) * 1e-3f, (float)k * 1e-3f);
+        b[k] = make_float2(0.5f, 0.25f + 1e-3f * k);
+    }
+    const float2 c = make_float2(1e-6f, 2e-6f);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            a[k] = __ffma2_rn(a[k], make_float2(-b[k].y, b[k].x), c);
+            b[k] = __ffma2_rn(b[k], make_float2(a[k].x, a[k].x), c);
+        }
+    }
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k < 4; k++) s = __fadd2_rn(s, __fadd2_rn(a[k], b[k]));
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
 }  // namespace
 
 template <typename T>
 void launch_fma_probe(T* out, int nblocks, int iters, cudaStream_t s) {
     k_fma_probe<T><<<nblocks, kBlock, 0, s>>>(out, iters, (T)0.999999, (T)1e-6);
 }
-void launch_ffma2_probe(void* out, int nblocks, int iters, cudaStream_t s) {
-    k_ffma2_probe<<<nblocks, kBlock, 0, s>>>(static_cast<float2*>(out), iters);
+void launch_ffma2_probe(void* out, int nblocks, int iters, bool selected_operands, cudaStream_t s) {
+    if (selected_operands) k_ffma2_sel_probe<<<nblocks, kBlock, 0, s>>>(static_cast<float2*>(out), iters);
+    else k_ffma2_probe<<<nblocks, kBlock, 0, s>>>(static_cast<float2*>(out), iters);
 }
 template void launch_fma_probe<float>(float*, int, int, cudaStream_t);
 template void launch_fma_probe<double>(double*, int, int, cudaStream_t);

@@ -755,7 +755,7 @@ int mag_compute_lambda(const double* q, const double* sigma, const double* u, in
 }
 
 int mag_probe_fma_peak(int precision, double* tflops) {
-    if (!tflops || precision < 0 || precision > 2) return MAG_ERR_ARG;
+    if (!tflops || precision < 0 || precision > 3) return MAG_ERR_ARG;
     int dev = 0, sms = 0;
     MAG_CUDA(cudaGetDevice(&dev));
     MAG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -770,7 +770,7 @@ int mag_probe_fma_peak(int precision, double* tflops) {
         cudaEventRecord(a, 0);
         if (precision == 0) launch_fma_probe<double>((double*)out, nblocks, iters, 0);
         else if (precision == 1) launch_fma_probe<float>((float*)out, nblocks, iters, 0);
-        else launch_ffma2_probe(out, nblocks, iters, 0);
+        else launch_ffma2_probe(out, nblocks, iters, precision == 3, 0);
         cudaEventRecord(b, 0);
         cudaEventSynchronize(b);
         float ms = 0.f;
@@ -782,7 +782,7 @@ int mag_probe_fma_peak(int precision, double* tflops) {
     cudaFree(out);
     MAG_CUDA(cudaGetLastError());
     // two flops per FMA; a packed f32x2 FMA is two FMAs
-    *tflops = (precision == 2 ? 4.0 : 2.0) * 8.0 * iters * (double)nblocks * 256 / (best * 1e-3) / 1e12;
+    *tflops = (precision >= 2 ? 4.0 : 2.0) * 8.0 * iters * (double)nblocks * 256 / (best * 1e-3) / 1e12;
     return MAG_OK;
 }
 

@@ -97,10 +97,114 @@ MAG_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
     return s;
 }
 
+// ------------------------------------------------- packed FP32 (sm_100a)
+// fma.rn.f32x2 does two FP32 FMAs in one instruction at the FMA pipe's rate
+// for two scalar FMAs, so it saves issue slots, not pipe time.
+// Complex sums s = sum_k x_k y_k are written on (re, im) pairs as
+//   T = sum_k (x.re, x.re) * (y.re, y.im),   U = sum_k (x.im, x.im) * (y.im, y.re),
+//   s = (T.re - U.re, T.im + U.im)   [one more packed FMA with the pair (-1, 1)]:
+// one factor is broadcast (its conjugation is a sign on the broadcast value),
+// the other is read as a pair in natural and swapped order; a conjugated
+// paired factor flips the sign of T.im and U.re at the combine.  A term costs
+// two packed FMAs instead of four scalar ones (two accumulators per element;
+// the single-accumulator form s += (x.re, x.re) (y.re, y.im) + (x.im, x.im)
+// (-y.im, y.re) measured slower in these kernels).  The sums are grouped
+// differently from the scalar chains, so results differ by FP32 rounding.
+#if defined(__CUDA_ARCH__)
+#define MAG_F32X2 1
+namespace f2 {
+__device__ __forceinline__ float2 nat(cplx<float> a) { return make_float2(a.re, a.im); }
+__device__ __forceinline__ float2 swp(cplx<float> a) { return make_float2(a.im, a.re); }
+__device__ __forceinline__ float2 bc(float x) { return make_float2(x, x); }
+__device__ __forceinline__ cplx<float> un(float2 v) { cplx<float> c; c.re = v.x; c.im = v.y; return c; }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+
+// T/U accumulation of one output element: s = sum_k op(x_k) op(y_k) with the
+// broadcast factor x (conjugated when CX) and the paired factor y (conjugated
+// when CY); ACC = 0: c = s, 1: c += s, -1: c -= s.  N terms.
+template <int N, bool CX, bool CY, int ACC>
+__device__ __forceinline__ cplx<float> dot(const cplx<float>* x, const cplx<float>* y, cplx<float> c) {
+    // result = T * tau + U * sigma, tau = (1, sy), sigma = (-sy, 1), sy = -1 when CY;
+    // the sign of the update is folded into the broadcasts.
+    constexpr float sg = ACC < 0 ? -1.f : 1.f;
+    constexpr float sxi = CX ? -1.f : 1.f;
+    float2 T, U;
+    if (ACC != 0 && !CY) T = nat(c);  // tau = (1, 1): T carries c
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+        const float2 br = bc(sg * x[k].re), bi = bc(sg * sxi * x[k].im);
+        if (k == 0 && !(ACC != 0 && !CY)) T = mul2(br, nat(y[k]));
+        else T = fma2(br, nat(y[k]), T);
+        if (k == 0) U = mul2(bi, swp(y[k]));
+        else U = fma2(bi, swp(y[k]), U);
+    }
+    if (!CY) return un(fma2(U, make_float2(-1.f, 1.f), T));
+    const float2 tau = make_float2(1.f, -1.f), sigma = make_float2(1.f, 1.f);
+    if (ACC == 0) return un(fma2(U, sigma, mul2(T, tau)));
+    return un(fma2(U, sigma, fma2(T, tau, nat(c))));
+}
+
+// rows [0, R) of c (=, +=, -=) op(a) op(b); the conjugated factor (if only
+// one is) is the broadcast one
+template <int R, int TA, int TB, int ACC>
+__device__ __forceinline__ void gemm(mat3<float>& c, const mat3<float>& a, const mat3<float>& b) {
+#pragma unroll
+    for (int i = 0; i < R; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            cplx<float> x[3], y[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                x[k] = TA ? a.e[k][i] : a.e[i][k];
+                y[k] = TB ? b.e[j][k] : b.e[k][j];
+            }
+            if (TB && !TA) c.e[i][j] = dot<3, true, false, ACC>(y, x, c.e[i][j]);
+            else c.e[i][j] = dot<3, TA != 0, TB != 0, ACC>(x, y, c.e[i][j]);
+        }
+}
+
+// conj(a b - c d), a and c broadcast
+__device__ __forceinline__ cplx<float> cross_conj(cplx<float> a, cplx<float> b, cplx<float> c, cplx<float> d) {
+    float2 T = mul2(bc(a.re), nat(b));
+    T = fma2(bc(-c.re), nat(d), T);
+    float2 U = mul2(bc(a.im), swp(b));
+    U = fma2(bc(-c.im), swp(d), U);
+    // a b - c d = (T.x - U.x, T.y + U.y), conjugated
+    return un(fma2(U, make_float2(-1.f, -1.f), mul2(T, make_float2(1.f, -1.f))));
+}
+
+// h op(xd) + z0 op(y0) + z1 op(y1) with h real (a Hermitian diagonal), the
+// entries of H broadcast and X paired (conjugated when CY); ACC as in dot
+template <bool CY, int ACC>
+__device__ __forceinline__ cplx<float> hdot(float h, cplx<float> xd, cplx<float> z0, cplx<float> y0, cplx<float> z1,
+                                            cplx<float> y1, cplx<float> c) {
+    constexpr float sg = ACC < 0 ? -1.f : 1.f;
+    float2 T;
+    if (ACC != 0 && !CY) T = fma2(bc(sg * h), nat(xd), nat(c));
+    else T = mul2(bc(sg * h), nat(xd));
+    T = fma2(bc(sg * z0.re), nat(y0), T);
+    T = fma2(bc(sg * z1.re), nat(y1), T);
+    float2 U = mul2(bc(sg * z0.im), swp(y0));
+    U = fma2(bc(sg * z1.im), swp(y1), U);
+    if (!CY) return un(fma2(U, make_float2(-1.f, 1.f), T));
+    const float2 tau = make_float2(1.f, -1.f), sigma = make_float2(1.f, 1.f);
+    if (ACC == 0) return un(fma2(U, sigma, mul2(T, tau)));
+    return un(fma2(U, sigma, fma2(T, tau, nat(c))));
+}
+}  // namespace f2
+#endif
+
 // rows [0, R) of  c = op(a) op(b)  (ACC = 0),  c += ...  (ACC = 1),  c -= ...  (ACC = -1);
 // TA / TB = 1 take the adjoint of a / b
 template <int R, int TA, int TB, int ACC, typename T>
 MAG_HD void gemm(mat3<T>& c, const mat3<T>& a, const mat3<T>& b) {
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+        f2::gemm<R, TA, TB, ACC>(c, a, b);
+        return;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < R; i++)
 #pragma unroll
@@ -146,6 +250,9 @@ MAG_HD void mul_sub(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 
 // 0, 1 of the left factor are read.
 template <typename T>
 MAG_HD cplx<T> cross_conj(cplx<T> a, cplx<T> b, cplx<T> c, cplx<T> d) {  // conj(a b - c d)
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) return f2::cross_conj(a, b, c, d);
+#endif
     cplx<T> s;
     s.re = a.re * b.re;
     s.re = fmaT(-a.im, b.im, s.re);
@@ -201,6 +308,15 @@ MAG_HD mat3<T> adj(const mat3<T>& a) {
 }
 template <typename T>
 MAG_HD void add_to(mat3<T>& a, const mat3<T>& b) {
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) a.e[i][j] = f2::un(__fadd2_rn(f2::nat(a.e[i][j]), f2::nat(b.e[i][j])));
+        return;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -208,6 +324,16 @@ MAG_HD void add_to(mat3<T>& a, const mat3<T>& b) {
 }
 template <typename T>
 MAG_HD void sub_from(mat3<T>& a, const mat3<T>& b) {
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+                a.e[i][j] = f2::un(f2::fma2(f2::bc(-1.f), f2::nat(b.e[i][j]), f2::nat(a.e[i][j])));
+        return;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -216,6 +342,15 @@ MAG_HD void sub_from(mat3<T>& a, const mat3<T>& b) {
 // a += s * b
 template <typename T>
 MAG_HD void axpy(mat3<T>& a, T s, const mat3<T>& b) {
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) a.e[i][j] = f2::un(f2::fma2(f2::bc(s), f2::nat(b.e[i][j]), f2::nat(a.e[i][j])));
+        return;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -235,6 +370,15 @@ MAG_HD void caxpy(mat3<T>& a, cplx<T> z, const mat3<T>& b) {
 template <typename T>
 MAG_HD mat3<T> scaled(const mat3<T>& a, T s) {
     mat3<T> c;
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) c.e[i][j] = f2::un(f2::mul2(f2::bc(s), f2::nat(a.e[i][j])));
+        return c;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -350,6 +494,24 @@ template <int SIDE, int TX, int ACC, typename T>
 MAG_HD void hgemm(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) {
     cplx<T> H[3][3];
     herm_rows(q, H);
+#ifdef MAG_F32X2
+    if constexpr (sizeof(T) == 4) {
+        // H broadcast, X paired
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int d = SIDE == 0 ? i : j;
+                const int k0 = d == 0 ? 1 : 0, k1 = d == 2 ? 1 : 2;  // the two indices != d
+                auto xe = [&](int r, int s) { return TX ? x.e[s][r] : x.e[r][s]; };  // op(X)_rs before conjugation
+                const cplx<T> xd = SIDE == 0 ? xe(d, j) : xe(i, d);
+                const cplx<T> z0 = SIDE == 0 ? H[i][k0] : H[k0][j], z1 = SIDE == 0 ? H[i][k1] : H[k1][j];
+                const cplx<T> y0 = SIDE == 0 ? xe(k0, j) : xe(i, k0), y1 = SIDE == 0 ? xe(k1, j) : xe(i, k1);
+                c.e[i][j] = f2::hdot<TX != 0, ACC>(H[d][d].re, xd, z0, y0, z1, y1, c.e[i][j]);
+            }
+        return;
+    }
+#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll

@@ -394,7 +394,7 @@ def compute_lambda(Q, SigmaP, U) -> np.ndarray:
 def probe_fma_peak(precision: str = "fp64") -> float:
     """Measured CUDA-core FMA throughput of the current device (TFLOP/s, 2 flops per FMA)."""
     v = ctypes.c_double()
-    code = {"fp64": 0, "fp32": 1, "fp32x2": 2}[precision]
+    code = {"fp64": 0, "fp32": 1, "fp32x2": 2, "fp32x2_selected": 3}[precision]
     check(_lib.load().mag_probe_fma_peak(code, ctypes.byref(v)), "mag_probe_fma_peak")
     return v.value
 

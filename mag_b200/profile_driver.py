@@ -124,7 +124,7 @@ def main(argv=None) -> int:
     if a.probe:
         from mag_b200.field_hmc import probe_fma_peak
 
-        out["fma_tflops"] = {p: probe_fma_peak(p) for p in ("fp64", "fp32", "fp32x2")}
+        out["fma_tflops"] = {p: probe_fma_peak(p) for p in ("fp64", "fp32", "fp32x2", "fp32x2_selected")}
     print(json.dumps(out))
     return 0
 
