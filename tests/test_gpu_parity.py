@@ -351,10 +351,13 @@ def test_mixed_precision_force_and_trajectory():
         with M.Chmc(dims, mag=2, n_stout=3, rho=0.1, n_steps=12, precision=prec, seed=5) as c:
             c.set_gauge(U)
             (r[prec],) = c.trajectory(True)
+    # the Hamiltonian is FP64 of the FP64 master links in both paths; the mixed MD moves the
+    # links by FP32 forces: the same accept decision, the plaquette within 1e-7, and Delta H
+    # within the FP32 force rounding of a hot start (5e-3 + 2e-3 |Delta H|)
     assert abs(r["mixed"]["h_old"] - r["fp64"]["h_old"]) <= 1e-12 * abs(r["fp64"]["h_old"])
-    assert abs(r["mixed"]["delta_h"] - r["fp64"]["delta_h"]) < 2e-2
-    assert abs(r["mixed"]["avg_plaquette"] - r["fp64"]["avg_plaquette"]) < 1e-5 or \
-        r["mixed"]["accept"] != r["fp64"]["accept"]
+    assert r["mixed"]["accept"] == r["fp64"]["accept"]
+    assert abs(r["mixed"]["delta_h"] - r["fp64"]["delta_h"]) < 5e-3 + 2e-3 * abs(r["fp64"]["delta_h"])
+    assert abs(r["mixed"]["avg_plaquette"] - r["fp64"]["avg_plaquette"]) < 1e-7
 
 
 def test_nan_is_reported_as_error_status():
