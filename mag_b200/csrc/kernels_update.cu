@@ -83,7 +83,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_evolve(DevGeom g, LinkPlanes<TU> 
     if (!locate(g, blockIdx.x * blockDim.x + threadIdx.x, ci, st)) return;
     const int mu = blockIdx.y;
     const int cc = constraint_case(ci, st, mu);
-    const int gm = nb(ci, st, mu, -1);
+    const int gm = nb_sel(ci, st, mu, -1);
     const mat3<TU> r = evolve_link<TU, TX>(Uin.load(mu, st.g), X, eps, cc, st.g, gm, mu);
     Uout.store(mu, st.g, r);
     if (Ucopy.p) Ucopy.store(mu, st.g, convert<float>(r));

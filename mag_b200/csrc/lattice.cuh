@@ -101,6 +101,21 @@ MAG_HD int nb(const ChainInfo& ci, const Site& st, int d1, int k1, int d2, int k
     return st.g + shift_off(ci, st.x[d1], d1, k1) + shift_off(ci, st.x[d2], d2, k2);
 }
 
+// a[d] for a direction d known only at run time, by selects.  Indexing the
+// arrays of ChainInfo and Site with a run-time d (as shift_off and nb do)
+// places both structs in local memory, so each neighbour address starts with
+// L1 loads.  In the staple, force and chain-rule kernels that measured faster
+// than selects (fewer registers); in the link update selects measured faster,
+// so it takes its neighbour from nb_sel.
+MAG_HD int at4(const int (&a)[4], int d) { return d == 0 ? a[0] : d == 1 ? a[1] : d == 2 ? a[2] : a[3]; }
+MAG_HD int nb_sel(const ChainInfo& ci, const Site& st, int d, int k) {
+    const int L = at4(ci.L, d), xd = at4(st.x, d);
+    int w = xd + k;
+    if (w >= L) w -= L;
+    else if (w < 0) w += L;
+    return st.g + (w - xd) * at4(ci.stride, d);
+}
+
 // lattice coordinate x3 of local x3 (a shard's halo and interior), and
 // whether a site belongs to the chain's own (interior) sites
 MAG_HD int x3_lattice(const ChainInfo& ci, int x3) {
@@ -124,7 +139,7 @@ MAG_HD int constraint_case(const ChainInfo& ci, const Site& st, int mu) {
         const int xi = i == 3 ? x3_lattice(ci, st.x[3]) : st.x[i];
         if (xi % m != 0) return 0;
     }
-    const int r = (mu == 3 ? x3_lattice(ci, st.x[3]) : st.x[mu]) % m;
+    const int r = (mu == 3 ? x3_lattice(ci, st.x[3]) : at4(st.x, mu)) % m;
     if (r == m - 1) return 100;
     if (r == 0) return 10;
     return 1;
