@@ -108,7 +108,10 @@ MAG_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
 // paired factor flips the sign of T.im and U.re at the combine.  A term costs
 // two packed FMAs instead of four scalar ones (two accumulators per element;
 // the single-accumulator form s += (x.re, x.re) (y.re, y.im) + (x.im, x.im)
-// (-y.im, y.re) measured slower in these kernels).  The sums are grouped
+// (-y.im, y.re) measured slower in these kernels).  The combine is FMA-pipe
+// work the scalar form does not do, so the short sums (the third-row
+// reconstruction of special-unitary products, the products with a Hermitian
+// factor) stay scalar: packed they measured slower.  The sums are grouped
 // differently from the scalar chains, so results differ by FP32 rounding.
 #if defined(__CUDA_ARCH__)
 #define MAG_F32X2 1
@@ -164,34 +167,6 @@ __device__ __forceinline__ void gemm(mat3<float>& c, const mat3<float>& a, const
         }
 }
 
-// conj(a b - c d), a and c broadcast
-__device__ __forceinline__ cplx<float> cross_conj(cplx<float> a, cplx<float> b, cplx<float> c, cplx<float> d) {
-    float2 T = mul2(bc(a.re), nat(b));
-    T = fma2(bc(-c.re), nat(d), T);
-    float2 U = mul2(bc(a.im), swp(b));
-    U = fma2(bc(-c.im), swp(d), U);
-    // a b - c d = (T.x - U.x, T.y + U.y), conjugated
-    return un(fma2(U, make_float2(-1.f, -1.f), mul2(T, make_float2(1.f, -1.f))));
-}
-
-// h op(xd) + z0 op(y0) + z1 op(y1) with h real (a Hermitian diagonal), the
-// entries of H broadcast and X paired (conjugated when CY); ACC as in dot
-template <bool CY, int ACC>
-__device__ __forceinline__ cplx<float> hdot(float h, cplx<float> xd, cplx<float> z0, cplx<float> y0, cplx<float> z1,
-                                            cplx<float> y1, cplx<float> c) {
-    constexpr float sg = ACC < 0 ? -1.f : 1.f;
-    float2 T;
-    if (ACC != 0 && !CY) T = fma2(bc(sg * h), nat(xd), nat(c));
-    else T = mul2(bc(sg * h), nat(xd));
-    T = fma2(bc(sg * z0.re), nat(y0), T);
-    T = fma2(bc(sg * z1.re), nat(y1), T);
-    float2 U = mul2(bc(sg * z0.im), swp(y0));
-    U = fma2(bc(sg * z1.im), swp(y1), U);
-    if (!CY) return un(fma2(U, make_float2(-1.f, 1.f), T));
-    const float2 tau = make_float2(1.f, -1.f), sigma = make_float2(1.f, 1.f);
-    if (ACC == 0) return un(fma2(U, sigma, mul2(T, tau)));
-    return un(fma2(U, sigma, fma2(T, tau, nat(c))));
-}
 }  // namespace f2
 #endif
 
@@ -250,9 +225,6 @@ MAG_HD void mul_sub(mat3<T>& acc, const mat3<T>& a, const mat3<T>& b) { gemm<3, 
 // 0, 1 of the left factor are read.
 template <typename T>
 MAG_HD cplx<T> cross_conj(cplx<T> a, cplx<T> b, cplx<T> c, cplx<T> d) {  // conj(a b - c d)
-#ifdef MAG_F32X2
-    if constexpr (sizeof(T) == 4) return f2::cross_conj(a, b, c, d);
-#endif
     cplx<T> s;
     s.re = a.re * b.re;
     s.re = fmaT(-a.im, b.im, s.re);
@@ -494,24 +466,6 @@ template <int SIDE, int TX, int ACC, typename T>
 MAG_HD void hgemm(mat3<T>& c, const herm8<T>& q, const mat3<T>& x) {
     cplx<T> H[3][3];
     herm_rows(q, H);
-#ifdef MAG_F32X2
-    if constexpr (sizeof(T) == 4) {
-        // H broadcast, X paired
-#pragma unroll
-        for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const int d = SIDE == 0 ? i : j;
-                const int k0 = d == 0 ? 1 : 0, k1 = d == 2 ? 1 : 2;  // the two indices != d
-                auto xe = [&](int r, int s) { return TX ? x.e[s][r] : x.e[r][s]; };  // op(X)_rs before conjugation
-                const cplx<T> xd = SIDE == 0 ? xe(d, j) : xe(i, d);
-                const cplx<T> z0 = SIDE == 0 ? H[i][k0] : H[k0][j], z1 = SIDE == 0 ? H[i][k1] : H[k1][j];
-                const cplx<T> y0 = SIDE == 0 ? xe(k0, j) : xe(i, k0), y1 = SIDE == 0 ? xe(k1, j) : xe(i, k1);
-                c.e[i][j] = f2::hdot<TX != 0, ACC>(H[d][d].re, xd, z0, y0, z1, y1, c.e[i][j]);
-            }
-        return;
-    }
-#endif
 #pragma unroll
     for (int i = 0; i < 3; i++)
 #pragma unroll
