@@ -37,27 +37,24 @@ MAG_HD mat3<T> staple_sum(const LinkPlanes<T>& U, const LinkPlanes<T>& W, const 
     const T c0 = IWASAKI ? (T)ci.c0 : T(1);
     const T c1 = (T)ci.c1;
     if (IWASAKI) {
-        mat3<T> acc;
-        set_zero(acc);
+        // the +mu (R1, R2) and -mu (R5, R6) groups in one loop, one accumulator each
+        mat3<T> accp, accm;
+        set_zero(accp);
+        set_zero(accm);
 #pragma unroll 1
         for (int nu = 0; nu < 4; nu++) {
             if (nu == mu) continue;
             mat3<T> t = mul_2r(U.load_rows01(nu, st.g), W.load(mu, nb(ci, st, nu, 1)));
-            add_to(acc, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 2))));
+            add_to(accp, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 2))));
             t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, nu, -1)), W.load(mu, nb(ci, st, nu, -1)));
-            add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 2, nu, -1))));
-        }
-        A = mul_nd(acc, U.load(mu, nb(ci, st, mu, 1)));
-        set_zero(acc);
-#pragma unroll 1
-        for (int nu = 0; nu < 4; nu++) {
-            if (nu == mu) continue;
-            mat3<T> t = mul_2r(U.load_rows01(nu, nb(ci, st, mu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, 1)));
-            add_to(acc, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
+            add_to(accp, mul_su3(t, U.load(nu, nb(ci, st, mu, 2, nu, -1))));
+            t = mul_2r(U.load_rows01(nu, nb(ci, st, mu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, 1)));
+            add_to(accm, mul_nd_su3(t, U.load(nu, nb(ci, st, mu, 1))));
             t = mul_dn_2r(U.load_cols01(nu, nb(ci, st, mu, -1, nu, -1)), W.load(mu, nb(ci, st, mu, -1, nu, -1)));
-            add_to(acc, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
+            add_to(accm, mul_su3(t, U.load(nu, nb(ci, st, mu, 1, nu, -1))));
         }
-        mul_dn_acc(A, U.load(mu, nb(ci, st, mu, -1)), acc);
+        A = mul_nd(accp, U.load(mu, nb(ci, st, mu, 1)));
+        mul_dn_acc(A, U.load(mu, nb(ci, st, mu, -1)), accm);
         A = scaled(A, c1);
     }
 #pragma unroll 1

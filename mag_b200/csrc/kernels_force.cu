@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kForceBlock) k_double_link(DevGeom g, LinkPlan
     Site st;
     int mu;
     if (!locate_link(g, ci, st, mu)) return;
-    W.store(mu, st.g, mul_su3(U.load(mu, st.g), U.load(mu, nb(ci, st, mu, 1))));
+    W.store(mu, st.g, mul_su3(U.load(mu, st.g), U.load(mu, nb_sel(ci, st, mu, 1))));
 }
 
 // F(x,mu) = i beta/3 TA(U(x,mu) A^dag)   (field-hmc.h:394-421, free-link case)
