@@ -113,7 +113,7 @@ MAG_HD cplx<T> cmul(cplx<T> a, cplx<T> b) {
 // reconstruction of special-unitary products, the products with a Hermitian
 // factor) stay scalar: packed they measured slower.  The sums are grouped
 // differently from the scalar chains, so results differ by FP32 rounding.
-#if defined(__CUDA_ARCH__)
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000
 #define MAG_F32X2 1
 namespace f2 {
 __device__ __forceinline__ float2 nat(cplx<float> a) { return make_float2(a.re, a.im); }
