@@ -10,7 +10,8 @@ levels rho = 0.1, sixteen force-gradient steps of tau = 1, constraint
 magnification 2, Metropolis accept: `value` is the plain FP64 path and the
 same lattice in mixed precision is measured beside it (`mixed`, with its
 speed-up over FP64).  On one GPU the default run also measures the 16^3 x 32
-FP64 configuration (12 FG steps) and the 96-chain ensemble as sub-keys.
+FP64 configuration (12 FG steps), the 96-chain ensemble and the 48^3 x 96 mixed
+configuration with Wilson loops (3 trajectories) as sub-keys.
 
   python bench.py [--gpus N --steps K --warmup W] [--workload NAME] [--impl reference]
 
@@ -427,12 +428,16 @@ def make_ctx(M, params, seed, precision, n_forced):
     return M.Chmc(params["dims"], seed=seed, **kw)
 
 
-def sub_run(M, workload: str, precisions, args) -> dict:
+def sub_run(M, workload: str, precisions, args, steps: int | None = None, warmup: int | None = None) -> dict:
     """One GPU, no collective: W forced-accept trajectories, then K timed ones (CUDA events around
-    the graph launches) per precision; chain-trajectories/s for an ensemble."""
+    the graph launches) per precision; chain-trajectories/s for an ensemble.  A workload with Wilson
+    loops measures them after every timed trajectory, inside the timed total."""
     import torch
 
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     params = workload_params(workload)
+    wl = params.get("wilson", 0)
     nchain = len(params["chains"]) if "chains" in params else 1
     out = {"workload": workload, "fg_steps": params["n_steps"], "stout_levels": params["n_stout"]}
     if "chains" in params:
@@ -441,18 +446,32 @@ def sub_run(M, workload: str, precisions, args) -> dict:
     else:
         out["lattice"] = "x".join(map(str, params["dims"]))
     for prec in precisions:
-        c = make_ctx(M, params, rank_seed(0), prec, args.warmup)
+        c = make_ctx(M, params, rank_seed(0), prec, warmup)
         c.hot_start(rank_seed(0))
-        if args.warmup:
-            c.run_chmc(args.warmup)
+        if warmup:
+            c.run_chmc(warmup)
         torch.cuda.synchronize()
-        recs = c.run_chmc(args.steps)
-        ms = c.last_run_ms()
-        out[prec] = {"value": nchain * args.steps / (ms / 1e3),
-                     "unit": "chain-traj/s" if nchain > 1 else "traj/s", "ms_per_step": ms / args.steps,
+        wl_ms = 0.0
+        if wl:
+            recs, ms = [], 0.0
+            for _ in range(steps):
+                recs += c.run_chmc(1)
+                ms += c.last_run_ms()
+                c.wilson_loops(wl, wl)
+                wl_ms += c.last_measure_ms()
+        else:
+            recs = c.run_chmc(steps)
+            ms = c.last_run_ms()
+        out[prec] = {"value": nchain * steps / ((ms + wl_ms) / 1e3),
+                     "unit": "chain-traj/s" if nchain > 1 else "traj/s", "ms_per_step": (ms + wl_ms) / steps,
+                     "steps": steps, "warmup": warmup,
                      "acceptance": statistics.fmean(r[k]["accept"] for r in recs for k in range(nchain)),
                      "delta_h_mean": statistics.fmean(r[k]["delta_h"] for r in recs for k in range(nchain)),
+                     "plaquette": recs[-1][0]["avg_plaquette"],
                      "graph_kernels_per_step": c.graph_kernel_count()}
+        if wl:
+            out[prec]["wilson_loops_ms_per_step"] = wl_ms / steps
+            out[prec]["wilson_share_of_step"] = wl_ms / (ms + wl_ms)
         c.close()
     if "fp64" in out and "mixed" in out:
         out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
@@ -652,6 +671,10 @@ def run_gpu(args, params, rank, world, dist):
     if world == 1 and args.workload == DEFAULT and not args.no_sub:
         sub["config2_16x16x16x32"] = sub_run(M, "16x16x16x32_iwasaki_3stout", ("fp64", "mixed"), args)
         sub["ensemble_96chains"] = sub_run(M, "ensemble_96chains", ("mixed",), args)
+        # 48^3 x 96 (10.6M sites, 72 GB in mixed precision): 4.4 s per trajectory, so 3 warm-up and 3
+        # timed trajectories, each followed by the Wilson loops R, T <= 8
+        sub["config5_48x48x48x96_wloops"] = sub_run(M, "48x48x48x96_iwasaki_3stout_wloops", ("mixed",), args,
+                                                    steps=min(args.steps, 3), warmup=min(args.warmup, 3))
 
     if rank != 0:
         return
