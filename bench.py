@@ -9,9 +9,10 @@ workload is the 32^4 lattice, Iwasaki beta = 2.25 (c1 = -0.331), three stout
 levels rho = 0.1, sixteen force-gradient steps of tau = 1, constraint
 magnification 2, Metropolis accept: `value` is the plain FP64 path and the
 same lattice in mixed precision is measured beside it (`mixed`, with its
-speed-up over FP64).  On one GPU the default run also measures the 16^3 x 32
-FP64 configuration (12 FG steps), the 96-chain ensemble and the 48^3 x 96 mixed
-configuration with Wilson loops (3 trajectories) as sub-keys.
+speed-up over FP64).  On one GPU the default run also measures the 8^4 thin-link
+demon configuration, the 16^3 x 32 FP64 configuration (12 FG steps), the 96-chain
+ensemble and the 48^3 x 96 mixed configuration with Wilson loops (3 trajectories)
+as sub-keys.
 
   python bench.py [--gpus N --steps K --warmup W] [--workload NAME] [--impl reference]
 
@@ -445,6 +446,9 @@ def sub_run(M, workload: str, precisions, args, steps: int | None = None, warmup
         out["sites"] = total_sites(params)
     else:
         out["lattice"] = "x".join(map(str, params["dims"]))
+    # FP64 links alone are 576 B per site
+    out["l2"] = ("working set > 126 MB L2" if total_sites(params) * 576 > 126e6
+                 else "working set inside the 126 MB L2 (no flush between trajectories)")
     for prec in precisions:
         c = make_ctx(M, params, rank_seed(0), prec, warmup)
         c.hot_start(rank_seed(0))
@@ -669,6 +673,7 @@ def run_gpu(args, params, rank, world, dist):
     # the other HMC configurations, measured beside the headline on one GPU
     sub = {}
     if world == 1 and args.workload == DEFAULT and not args.no_sub:
+        sub["config1_8x8x8x8_thin_demon"] = sub_run(M, "8x8x8x8_iwasaki_thin", ("fp64",), args)
         sub["config2_16x16x16x32"] = sub_run(M, "16x16x16x32_iwasaki_3stout", ("fp64", "mixed"), args)
         sub["ensemble_96chains"] = sub_run(M, "ensemble_96chains", ("mixed",), args)
         # 48^3 x 96 (10.6M sites, 72 GB in mixed precision): 4.4 s per trajectory, so 3 warm-up and 3
