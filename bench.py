@@ -446,11 +446,11 @@ def sub_run(M, workload: str, precisions, args, steps: int | None = None, warmup
         out["sites"] = total_sites(params)
     else:
         out["lattice"] = "x".join(map(str, params["dims"]))
-    # FP64 links alone are 576 B per site
-    out["l2"] = ("working set > 126 MB L2" if total_sites(params) * 576 > 126e6
-                 else "working set inside the 126 MB L2 (no flush between trajectories)")
     for prec in precisions:
         c = make_ctx(M, params, rank_seed(0), prec, warmup)
+        dev = c.device_bytes()  # the context's fields, touched by every trajectory
+        out["l2"] = (f"working set {dev / 1e9:.2f} GB > 126 MB L2" if dev > 126e6
+                     else f"working set {dev / 1e6:.0f} MB inside the 126 MB L2 (no flush between trajectories)")
         c.hot_start(rank_seed(0))
         if warmup:
             c.run_chmc(warmup)
