@@ -3,7 +3,10 @@
 //   * div_by for every divisor 2..4096 on dividends spread over [0, 2^31) and
 //     on every value near multiples of the divisor;
 //   * decode of every site of a set of lattice shapes (odd, even, powers of two,
-//     the 48^3 x 96 workload's extents) against % and /.
+//     the 48^3 x 96 workload's extents) against % and /;
+//   * on the same shapes, every site's neighbour index along each direction at
+//     steps -2..2 from nb (dynamically indexed) and nb_sel (selects) against the
+//     index of the wrapped coordinates.
 // Prints "ok" and exits 0, or prints the first mismatch and exits 1.
 #include <cstdio>
 #include <cstdint>
@@ -60,6 +63,18 @@ static int check_lattice(int L0, int L1, int L2, int L3) {
                         st.x[0], st.x[1], st.x[2], st.x[3], x[0], x[1], x[2], x[3]);
             return 1;
         }
+        for (int d = 0; d < 4; d++)
+            for (int k = -2; k <= 2; k++) {
+                int y[4] = {x[0], x[1], x[2], x[3]};
+                y[d] = ((y[d] + k) % L[d] + L[d]) % L[d];
+                const long want = ci.off + y[0] + (long)L[0] * (y[1] + (long)L[1] * (y[2] + (long)L[2] * y[3]));
+                const int a = nb(ci, st, d, k), b = nb_sel(ci, st, d, k);
+                if (a != want || b != want) {
+                    std::printf("neighbour of %ld along %d by %d on %dx%dx%dx%d: nb %d, nb_sel %d, expected %ld\n",
+                                s, d, k, L0, L1, L2, L3, a, b, want);
+                    return 1;
+                }
+            }
     }
     return 0;
 }

@@ -1,7 +1,8 @@
 """The library's site decode (mag_b200/csrc/lattice.cuh) built for the host with g++:
 its multiply-shift division by the chain extents against plain division, for
 divisors 2..4096 and large ones on dividends across [0, 2^31), and every site of a
-set of lattice shapes (tests/cpp/decode_check.cpp)."""
+set of lattice shapes; on those shapes the neighbour indices of nb and nb_sel at steps
+-2..2 along every direction (tests/cpp/decode_check.cpp)."""
 import os
 import subprocess
 
