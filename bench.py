@@ -429,6 +429,23 @@ def make_ctx(M, params, seed, precision, n_forced):
     return M.Chmc(params["dims"], seed=seed, **kw)
 
 
+def measured_hbm_gbs() -> float:
+    """MEASURED_PEAKS.json's copy bandwidth of this pool's B200s, else the earlier measurement 6.65 TB/s."""
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        return float(json.load(open(pp)).get("hbm_gbs", 6650.0))
+    return 6650.0
+
+
+def wilson_bytes(wl: int, V: int) -> int:
+    """Algorithmic HBM bytes of one Wilson-loop measurement (R, T <= wl, three spatial directions) of V
+    sites: per direction the R-line planes (first: read U, write the line; then read U and the previous
+    line, write), per T the temporal line (the same) and the accumulation pass (reads the wl S-line
+    planes and the temporal line once per site; the shifted reads come from L2)."""
+    per_dir = (288 + (wl - 1) * 432) + (288 + (wl - 1) * 432) + wl * (wl + 1) * 144
+    return 3 * per_dir * V
+
+
 def sub_run(M, workload: str, precisions, args, steps: int | None = None, warmup: int | None = None) -> dict:
     """One GPU, no collective: W forced-accept trajectories, then K timed ones (CUDA events around
     the graph launches) per precision; chain-trajectories/s for an ensemble.  A workload with Wilson
@@ -476,6 +493,10 @@ def sub_run(M, workload: str, precisions, args, steps: int | None = None, warmup
         if wl:
             out[prec]["wilson_loops_ms_per_step"] = wl_ms / steps
             out[prec]["wilson_share_of_step"] = wl_ms / (ms + wl_ms)
+            hbm = measured_hbm_gbs()
+            wach = wilson_bytes(wl, total_sites(params)) / (wl_ms / steps * 1e-3) / 1e9
+            out[prec]["wilson_hbm"] = {"achieved": wach, "peak": hbm, "unit": "GB/s", "frac": wach / hbm,
+                                       "bytes_per_measurement": wilson_bytes(wl, total_sites(params))}
         c.close()
     if "fp64" in out and "mixed" in out:
         out["mixed"]["speedup_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
@@ -585,7 +606,7 @@ def run_gpu(args, params, rank, world, dist):
     pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(pp):
         peaks = json.load(open(pp))
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    hbm_peak = measured_hbm_gbs()
     roofline["evolve_hbm"] = {"achieved": bytes_evolve / (ev_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                               "frac": bytes_evolve / (ev_ms * 1e-3) / 1e9 / hbm_peak,
                               "peak_source": ("MEASURED_PEAKS.json hbm_gbs" if "hbm_gbs" in peaks
@@ -702,12 +723,8 @@ def run_gpu(args, params, rank, world, dist):
         line["other_configs"] = sub
     if wl:
         line["wilson_loops_ms_per_step"] = wl_ms / args.steps
-        # HBM roofline of one Wilson-loop measurement (R, T <= wl, three spatial directions): per direction
-        # the R-line planes (first: read U, write the line; then read U and the previous line, write), per T
-        # the temporal line (the same) and the accumulation pass (reads the wl S-line planes and the
-        # temporal line once per site; the shifted reads come from L2)
-        per_dir = (288 + (wl - 1) * 432) + (288 + (wl - 1) * 432) + wl * (wl + 1) * 144
-        wbytes = 3 * per_dir * V
+        # HBM roofline of one Wilson-loop measurement (bytes as wilson_bytes counts them)
+        wbytes = wilson_bytes(wl, V)
         wach = wbytes / (wl_ms / args.steps * 1e-3) / 1e9
         line["wilson_hbm"] = {"achieved": wach, "peak": hbm_peak, "unit": "GB/s", "frac": wach / hbm_peak,
                               "bytes_per_measurement": wbytes,
